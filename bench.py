@@ -1,0 +1,270 @@
+"""Benchmark: Mpts/s of bit-exact 3D Delaunay triangulation on B200.
+
+Workload (one step = one full triangulation): the 1,000,000-point mixed cloud
+(half uniform in [0,1)^3, half N(0.5, 0.1^2) clipped), FP64, PBA grid 512^3.
+
+  value  device throughput: points already in HBM, tetrahedra left in HBM
+  e2e    the public API with pinned host buffers: H2D of the points and D2H of
+         all tetrahedra inside every timed step
+  roofline  the PBA phase (HBM-bound) measured with CUDA events on the
+         library's stream: algorithmic bytes 20*G^3 per launch set (z pass
+         writes 4 B/voxel, y and x passes read and write 4 B/voxel)
+  cpu_baseline  the CPU oracle (a C restatement of the same pipeline, OpenMP over
+         all host cores) on a bounded sample of the same distribution
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+With N > 1 (torchrun) every rank triangulates its own cloud: replicas, weak
+scaling; the time is the max over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+import numpy as np  # noqa: E402
+
+WORKLOAD = {"workload": "mixed-1M", "points": 1_000_000, "grid": 512,
+            "distribution": "50% U[0,1)^3 + 50% N(0.5,0.1^2) clipped, FP64", "seed": 1}
+METRIC = "Mpts/s to bit-exact 3D DT on 1 B200"
+SAMPLE_POINTS, SAMPLE_GRID = 125_000, 256  # same voxel density (134 voxels/point)
+
+
+def _peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_run(steps, threads):
+    """The oracle on the bounded sample; returns (Mpts/s, seconds per run)."""
+    from oracle import oracle_py
+    from gstar4d_b200 import workloads
+    oracle_py.build() if not os.path.exists(oracle_py.LIB_PATH) else None
+    pts = workloads.mixed(SAMPLE_POINTS, seed=WORKLOAD["seed"])
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        oracle_py.triangulate(pts, SAMPLE_GRID, threads=threads)
+        times.append(time.perf_counter() - t0)
+    t = statistics.median(times)
+    return len(pts) / t / 1e6, t, len(pts)
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    for _ in range(max(0, min(args.warmup, 1))):
+        cpu_run(1, threads)
+    v, t, n = cpu_run(max(1, args.steps), threads)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(v, 4), "unit": "Mpts/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": dict(WORKLOAD),
+        "cpu_baseline": {"value": round(v, 4), "unit": "Mpts/s", "cores": threads, "kind": "port",
+                         "sample": "%d-point mixed cloud at grid %d^3 (same distribution and voxel density), "
+                                   "median of %d runs" % (n, SAMPLE_GRID, max(1, args.steps))},
+        "e2e": {"value": round(v, 4), "unit": "Mpts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--points", type=int, default=WORKLOAD["points"])
+    ap.add_argument("--grid", type=int, default=WORKLOAD["grid"])
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return reference_arm(args)
+
+    import torch
+    import torch.distributed as dist
+    import gstar4d_b200
+    from gstar4d_b200 import workloads
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    cfg = dict(WORKLOAD)
+    cfg["points"], cfg["grid"] = args.points, args.grid
+    pts = workloads.mixed(args.points, seed=WORKLOAD["seed"] + rank)
+    n = len(pts)
+    tri = gstar4d_b200.Triangulator(grid_size=args.grid, device=local)
+    ext = torch.cuda.ExternalStream(tri.stream, device=local)
+    d_pts = torch.from_numpy(pts).to(f"cuda:{local}")
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device=f"cuda:{local}")  # 256 MB > L2
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- device throughput (value) ----
+    for _ in range(args.warmup):
+        tri.triangulate_device(d_pts.data_ptr(), n)
+    barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    step_ms, pba_ms, launches, ntets = [], [], 0, 0
+    for _ in range(args.steps):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(ext)
+        _, ntets, st = tri.triangulate_device(d_pts.data_ptr(), n)
+        e.record(ext)
+        e.synchronize()
+        step_ms.append(s.elapsed_time(e))
+        pba_ms.append(st["t_pba_ms"])
+        launches += st["gpu_launches"]
+        last = st
+    barrier()
+    clocks = sampler.stop()
+    total_ms = sum(step_ms)
+    if world > 1:
+        t = torch.tensor([total_ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * n * args.steps / (total_ms / 1e3) / 1e6
+
+    # ---- end to end through the public API with pinned host buffers ----
+    h_pts = torch.from_numpy(pts).pin_memory()
+    cap = int(ntets * 1.2) + 1024
+    h_out = torch.empty((cap, 8), dtype=torch.int32).pin_memory()
+    out_np = h_out.numpy().view(gstar4d_b200.TET_DTYPE).reshape(-1)
+    pts_np = h_pts.numpy()
+    for _ in range(max(1, min(args.warmup, 2))):
+        tri.triangulate(pts_np, out=out_np)
+    barrier()
+    e2e_ms = []
+    for _ in range(args.steps):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(ext)
+        tets, _, _ = tri.triangulate(pts_np, out=out_np)
+        e.record(ext)
+        e.synchronize()
+        e2e_ms.append(s.elapsed_time(e))
+    e2e_total = sum(e2e_ms)
+    if world > 1:
+        t = torch.tensor([e2e_total], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    e2e = world * n * args.steps / (e2e_total / 1e3) / 1e6
+
+    if rank == 0:
+        peak, peak_kind = _peaks()
+        G = args.grid
+        alg_bytes = 20.0 * G ** 3
+        pba_avg = statistics.mean(pba_ms)
+        achieved = alg_bytes / (pba_avg / 1e3) / 1e9
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "Mpts/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(cfg, l2="256 MB buffer written between timed steps", parallelism="replicas"),
+            "e2e": {"value": round(e2e, 3), "unit": "Mpts/s", "h2d_bytes_per_step": int(n * 24),
+                    "d2h_bytes_per_step": int(len(tets) * 32)},
+            "roofline": {"kernel": "pba (z,y,x passes)", "bound": "hbm", "achieved": round(achieved, 1),
+                         "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                         "traffic": None, "algorithmic_bytes": alg_bytes, "avg_ms": round(pba_avg, 4)},
+            "stages_ms": {k: round(last[k], 3) for k in ("t_init_ms", "t_pba_ms", "t_star_ms", "t_splay_ms",
+                                                          "t_out_ms", "t_total_ms")},
+            "splay": {"loops": last["loops"], "insertions": last["splay_insertions"], "proofs": last["proofs"],
+                      "exact_predicates": last["exact_predicates"], "tets": ntets},
+            "clocks": clocks,
+            "gpu_launches": int(launches),
+        }
+        if not args.no_cpu:
+            threads = os.cpu_count() or 1
+            v, t, ns = cpu_run(1, threads)
+            line["cpu_baseline"] = {"value": round(v, 4), "unit": "Mpts/s", "cores": threads, "kind": "port",
+                                    "sample": "%d-point mixed cloud at grid %d^3 (same distribution and voxel "
+                                              "density), one run" % (ns, SAMPLE_GRID)}
+        print(json.dumps(line))
+    tri.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,165 @@
+// Internal layouts and launch declarations of the B200 gStar4D pipeline.
+//
+// HBM layout (n points, G^3 grid):
+//   P        double4[n]     points in Morton order (x,y,z,0): one 32-byte sector each
+//   vox      uint32[n]      voxel of each point, packed x | y<<10 | z<<20
+//   grid A/B uint32[G^3]    digital Voronoi sites, packed voxel coords, x fastest
+//   hh       int32[n*256]   per-star history hash: every point ever inserted in the
+//                           star (bit 31 = currently in the link), open addressing
+//   tri      uint2[n*256]   per-star link triangles, 8 bytes each (see TriPack)
+//   hdr      StarHdr[n]     triangle count, history count, pass number, flags
+//   bucket   int32[n*64]    initial candidate worksets (Voronoi pairs + missing)
+//   inbox    int32[n*64]    insertion requests for the next splaying round
+#pragma once
+
+#ifndef G4D_HOST_EMULATION
+#include <cuda_runtime.h>
+#endif
+
+#include <cstdint>
+
+#include "gstar4d.h"
+
+// Dynamic shared memory declaration (a host build of the warp kernels for
+// unit testing supplies its own definition).
+#ifndef G4D_DYN_SMEM
+#define G4D_DYN_SMEM(name) extern __shared__ unsigned char name[]
+#endif
+// Error-site tracing hook (empty on the device; the host build prints).
+#ifndef G4D_TRACE
+#define G4D_TRACE(...) ((void)0)
+#endif
+
+namespace g4d {
+
+constexpr uint32_t MARKER = 0xffffffffu;  // voxel without a site
+constexpr int HSLOTS = 512;               // history hash slots per star
+constexpr int HMAX = 255;                 // max history entries (hash load <= 1/2)
+constexpr int TMAX = 252;                 // max link triangles (2 * HMAX - 4)
+constexpr int TSTRIDE = 256;              // triangle slots per star in HBM
+constexpr int BUCKET_CAP = 64;            // initial candidates kept per star
+constexpr int INBOX_CAP = 64;             // insertion requests per star per round
+constexpr int MIN_WORKSET = 8;            // GDelCommon.h:49
+constexpr uint32_t HEMPTY = 0x7fffffffu;
+constexpr uint32_t HLINK = 0x80000000u;
+constexpr uint32_t HID = 0x7fffffffu;
+
+// error bits (device error word)
+enum : unsigned {
+    ERR_PRECISION = 1u,
+    ERR_CAPACITY = 2u,
+    ERR_TOPOLOGY = 4u,   // a hole that is not a disk, or every triangle beneath
+    ERR_PROOF = 8u,      // no containment proof found
+    ERR_DROWNCAP = 16u,  // drowned list full
+};
+
+// star header flags
+enum : uint8_t { HDR_EMIT_ALL = 1, HDR_BUILT = 2 };
+
+struct StarHdr {
+    uint8_t ntri, nhist, pass, flags;
+};
+
+// device counters (one struct in HBM, read by the host once per round)
+struct Counters {
+    int ins_count;        // stars queued for insertion
+    int emit_next;        // stars queued for emission next round
+    int drown_next;       // drowned items for next round
+    int overflow;         // inbox overflow happened
+    unsigned err;         // ERR_* bits
+    unsigned exact;       // exact predicate evaluations
+    unsigned long long insertions;
+    unsigned long long drowned_total;
+    unsigned long long proofs_total;
+    int tet_count;
+    int dbg_set;          // first failing exact-predicate input recorded below
+    double dbg_pts[15];
+    int dbg_ids[5];
+};
+
+__host__ __device__ inline uint32_t enc_vox(uint32_t x, uint32_t y, uint32_t z) { return x | (y << 10) | (z << 20); }
+__host__ __device__ inline uint32_t vx(uint32_t e) { return e & 1023u; }
+__host__ __device__ inline uint32_t vy(uint32_t e) { return (e >> 10) & 1023u; }
+__host__ __device__ inline uint32_t vz(uint32_t e) { return (e >> 20) & 1023u; }
+
+__device__ __forceinline__ uint32_t hslot0(int v) { return ((uint32_t)v * 2654435761u) >> 23; }
+
+// Triangle packing in HBM (8 bytes):
+//   x = v0 | v1<<9 | v2<<18 | gen<<27 | kept<<31
+//   y = o0 | o1<<8 | o2<<16 | j0<<24 | j1<<26 | j2<<28
+// v* are history slots (9 bits); o* the adjacent triangle across the edge
+// opposite v*; j* the position of the shared edge inside that neighbour;
+// gen = creation pass (4 bits, 1..15); kept = lower-hull tetra at extraction.
+constexpr uint32_t TRI_KEPT = 0x80000000u;
+__device__ __forceinline__ int tri_v(uint2 T, int i) { return (int)((T.x >> (9 * i)) & 511u); }
+__device__ __forceinline__ int tri_gen(uint2 T) { return (int)((T.x >> 27) & 15u); }
+__device__ __forceinline__ int tri_o(uint2 T, int i) { return (int)((T.y >> (8 * i)) & 255u); }
+__device__ __forceinline__ int tri_j(uint2 T, int i) { return (int)((T.y >> (24 + 2 * i)) & 3u); }
+__device__ __forceinline__ uint2 tri_pack(int v0, int v1, int v2, int gen, int o0, int o1, int o2, int j0, int j1,
+                                          int j2) {
+    uint2 T;
+    T.x = (uint32_t)v0 | ((uint32_t)v1 << 9) | ((uint32_t)v2 << 18) | ((uint32_t)(gen & 15) << 27);
+    T.y = (uint32_t)o0 | ((uint32_t)o1 << 8) | ((uint32_t)o2 << 16) | ((uint32_t)j0 << 24) | ((uint32_t)j1 << 26) |
+          ((uint32_t)j2 << 28);
+    return T;
+}
+
+struct Dev {
+    int n, G;
+    const double4* P;
+    const uint32_t* vox;
+    const uint32_t* mkey;  // Morton keys, sorted
+    const uint32_t* ckey;  // column-sorted voxel keys ((y*G+x)<<10 | z)
+    const int* cid;        // column-sorted point ids
+    const int* colStart;   // [G*G]
+    const int* colEnd;     // [G*G]
+    int* hh;
+    uint2* tri;
+    StarHdr* hdr;
+    int* bucket;
+    int* bucketCount;
+    int* inbox;
+    int* inboxCount;
+    int* wlIns;
+    int* wlEmit;
+    int* wlEmitNext;
+    int2* drown;
+    int2* drownNext;
+    int drownCap;
+    Counters* ctr;
+};
+
+// ---- launchers (host) --------------------------------------------------------
+struct Launch {
+    cudaStream_t stream;
+    long long* launches;  // incremented per kernel launch
+};
+
+// order
+void launch_minmax(const Launch& L, const double* xyz, int n, unsigned long long* mm);
+void launch_scale_morton(const Launch& L, const double* xyz, const double* scaled_in, int n, int G,
+                         const unsigned long long* mm, uint32_t* keys, int* vals, uint32_t* vox_in, unsigned* err);
+void launch_gather(const Launch& L, const double* xyz, const uint32_t* vox_in, const int* order, int n,
+                   double4* P, uint32_t* vox, int* sorted_to_input);
+void launch_colkeys(const Launch& L, const uint32_t* vox, int n, int G, uint32_t* ckey, int* cid);
+void launch_colranges(const Launch& L, const uint32_t* ckey, int n, int G, int* colStart, int* colEnd);
+
+// pba
+void launch_pba_z(const Launch& L, const Dev& D, uint32_t* out);
+void launch_pba_y(const Launch& L, int G, const uint32_t* in, uint32_t* out);
+void launch_pba_x(const Launch& L, int G, const uint32_t* in, uint32_t* out);
+void launch_pairs(const Launch& L, const Dev& D, const uint32_t* grid);
+void launch_missing(const Launch& L, const Dev& D);
+
+// stars
+void launch_star_build(const Launch& L, const Dev& D);
+void launch_star_insert(const Launch& L, const Dev& D, int count);
+void launch_emit(const Launch& L, const Dev& D, int count);
+void launch_proof(const Launch& L, const Dev& D, int count);
+void launch_check(const Launch& L, const Dev& D, unsigned long long* bad);
+void launch_tet_count(const Launch& L, const Dev& D, int* cnt);
+void launch_tet_write(const Launch& L, const Dev& D, const int* base, g4d_tet* tets, const int* sorted_to_input);
+void launch_eval_pred(const Launch& L, int kind, const double* pts, const int* idx, int count, int8_t* out,
+                      unsigned* err);
+
+}  // namespace g4d

@@ -1,0 +1,148 @@
+// Input scaling, Morton keys and the sorted point layout.
+//
+// Restates Application::_scalePoint (Main/Application.cpp:589-603: one min and
+// max over all coordinates, p -> 1 + (G-3)(p-min)/(max-min)) and the Morton
+// order of PointData::init (GDelaunay/GDelData.cu:51-134: 10 bits per axis,
+// x in bit 0, stable sort). The Morton positions are the Simulation-of-
+// Simplicity ranks, so the arithmetic here is IEEE round-to-nearest with no
+// contraction, identical to the reference's host-side double evaluation.
+#include "g4d_internal.cuh"
+
+namespace g4d {
+
+__device__ __forceinline__ unsigned long long dkey(double v) {
+    const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+    return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double dkey_inv(unsigned long long k) {
+    const unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+    return __longlong_as_double((long long)b);
+}
+
+__global__ void k_minmax(const double* __restrict__ xyz, long long m, unsigned long long* mm) {
+    unsigned long long lo = ~0ull, hi = 0ull;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < m; i += (long long)gridDim.x * blockDim.x) {
+        const unsigned long long k = dkey(xyz[i]);
+        lo = k < lo ? k : lo;
+        hi = k > hi ? k : hi;
+    }
+    for (int o = 16; o; o >>= 1) {
+        const unsigned long long a = __shfl_xor_sync(0xffffffffu, lo, o);
+        const unsigned long long b = __shfl_xor_sync(0xffffffffu, hi, o);
+        lo = a < lo ? a : lo;
+        hi = b > hi ? b : hi;
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(&mm[0], lo);
+        atomicMax(&mm[1], hi);
+    }
+}
+
+__device__ __forceinline__ uint32_t spread10(uint32_t v) {
+    v = (v | (v << 16)) & 0x030000FFu;
+    v = (v | (v << 8)) & 0x0300F00Fu;
+    v = (v | (v << 4)) & 0x030C30C3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+
+// mode: mm != nullptr -> scale xyz with the global min/max; else grid_src holds
+// grid coordinates (the reference's scaled points, or points already in grid units).
+__global__ void k_scale_morton(const double* __restrict__ xyz, const double* __restrict__ grid_src, int n, int G,
+                               const unsigned long long* __restrict__ mm, uint32_t* __restrict__ keys,
+                               int* __restrict__ vals, uint32_t* __restrict__ vox_in, unsigned* err) {
+    double mn = 0.0, rng = 1.0;
+    if (mm) {
+        mn = dkey_inv(mm[0]);
+        rng = __dsub_rn(dkey_inv(mm[1]), mn);
+    }
+    const double g3 = (double)(G - 3);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t q[3];
+        for (int c = 0; c < 3; ++c) {
+            double t;
+            if (mm) {
+                t = __dsub_rn(xyz[3 * (size_t)i + c], mn);
+                t = __dmul_rn(g3, t);
+                t = __ddiv_rn(t, rng);
+                t = __dadd_rn(t, 1.0);
+            } else {
+                t = grid_src[3 * (size_t)i + c];
+            }
+            int v = (int)t;
+            if (!(t >= 1.0) || v > G - 2) {
+                atomicOr(err, 0x100u);  // coordinates outside [1, G-2]
+                v = v < 1 ? 1 : (v > G - 2 ? G - 2 : v);
+            }
+            q[c] = (uint32_t)v;
+        }
+        keys[i] = spread10(q[0]) | (spread10(q[1]) << 1) | (spread10(q[2]) << 2);
+        vals[i] = i;
+        vox_in[i] = enc_vox(q[0], q[1], q[2]);
+    }
+}
+
+__global__ void k_gather(const double* __restrict__ xyz, const uint32_t* __restrict__ vox_in,
+                         const int* __restrict__ order, int n, double4* __restrict__ P, uint32_t* __restrict__ vox,
+                         int* __restrict__ sorted_to_input) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int s = order[i];
+        P[i] = make_double4(xyz[3 * (size_t)s], xyz[3 * (size_t)s + 1], xyz[3 * (size_t)s + 2], 0.0);
+        vox[i] = vox_in[s];
+        if (sorted_to_input) sorted_to_input[i] = s;
+    }
+}
+
+__global__ void k_colkeys(const uint32_t* __restrict__ vox, int n, int G, uint32_t* __restrict__ ckey,
+                          int* __restrict__ cid) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t e = vox[i];
+        ckey[i] = ((vy(e) * (uint32_t)G + vx(e)) << 10) | vz(e);
+        cid[i] = i;
+    }
+}
+
+__global__ void k_colranges(const uint32_t* __restrict__ ckey, int n, int* __restrict__ cs, int* __restrict__ ce) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t c = ckey[i] >> 10;
+        if (i == 0 || (ckey[i - 1] >> 10) != c) cs[c] = i;
+        if (i == n - 1 || (ckey[i + 1] >> 10) != c) ce[c] = i + 1;
+    }
+}
+
+static int blocks_for(long long work, int threads) {
+    long long b = (work + threads - 1) / threads;
+    const long long cap = 148LL * 16;
+    if (b > cap) b = cap;
+    return (int)(b < 1 ? 1 : b);
+}
+
+void launch_minmax(const Launch& L, const double* xyz, int n, unsigned long long* mm) {
+    k_minmax<<<blocks_for(3LL * n, 256), 256, 0, L.stream>>>(xyz, 3LL * n, mm);
+    ++*L.launches;
+}
+
+void launch_scale_morton(const Launch& L, const double* xyz, const double* grid_src, int n, int G,
+                         const unsigned long long* mm, uint32_t* keys, int* vals, uint32_t* vox_in, unsigned* err) {
+    k_scale_morton<<<blocks_for(n, 256), 256, 0, L.stream>>>(xyz, grid_src, n, G, mm, keys, vals, vox_in, err);
+    ++*L.launches;
+}
+
+void launch_gather(const Launch& L, const double* xyz, const uint32_t* vox_in, const int* order, int n, double4* P,
+                   uint32_t* vox, int* sorted_to_input) {
+    k_gather<<<blocks_for(n, 256), 256, 0, L.stream>>>(xyz, vox_in, order, n, P, vox, sorted_to_input);
+    ++*L.launches;
+}
+
+void launch_colkeys(const Launch& L, const uint32_t* vox, int n, int G, uint32_t* ckey, int* cid) {
+    k_colkeys<<<blocks_for(n, 256), 256, 0, L.stream>>>(vox, n, G, ckey, cid);
+    ++*L.launches;
+}
+
+void launch_colranges(const Launch& L, const uint32_t* ckey, int n, int G, int* colStart, int* colEnd) {
+    (void)G;
+    k_colranges<<<blocks_for(n, 256), 256, 0, L.stream>>>(ckey, n, colStart, colEnd);
+    ++*L.launches;
+}
+
+}  // namespace g4d

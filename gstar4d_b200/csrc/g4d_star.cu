@@ -1,0 +1,1014 @@
+// Stars and star splaying.
+//
+// A star is the link of a point in the 4D convex hull of the points lifted to
+// (x, y, z, |p|^2): a triangulated 2-sphere of neighbour points (the reference's
+// StarData, GDelaunay/GDelData.h:54-85, GDelCommon.h:598-717). The reference
+// updates stars with one launch per insertion index across all stars
+// (GDelHost.cu:591-743, 1208-1360). Here one warp owns one star for a whole
+// round: it stages the star's history hash, coordinates and triangles in shared
+// memory, inserts every pending point (beneath test = orient4 < 0 as in
+// GDelPredKernels.cu:233-420; hole re-fan as in GDelKernels.cu:622-783) and
+// writes the star back once. Between rounds, emission (GDelKernels.cu:818-939)
+// and containment proofs (GDelPredKernels.cu:427-538) queue insertions into
+// per-star inboxes; the loop ends when no star receives a new point.
+#include "g4d_internal.cuh"
+#include "g4d_predicates.cuh"
+
+namespace g4d {
+
+constexpr int WARPS_PER_BLOCK = 4;
+
+// Per-warp shared-memory image of one star (about 16 KB).
+struct WS {
+    int hh[HSLOTS];                // history hash: point id | link bit, HEMPTY when free
+    uint8_t cix[HSLOTS];           // slot -> index into the coordinate cache
+    double cx[HMAX + 1], cy[HMAX + 1], cz[HMAX + 1];
+    uint16_t tv[3][TSTRIDE];       // triangle vertices (history slots)
+    uint8_t to[3][TSTRIDE];        // neighbour across the edge opposite each vertex
+    uint8_t tj[3][TSTRIDE];        // position of the shared edge inside that neighbour
+    uint8_t tf[TSTRIDE];           // bit 7 alive, bits 0..3 creation pass
+    uint8_t efrom[HSLOTS], eto[HSLOTS];
+    uint32_t erec[TSTRIDE];        // hole boundary edges
+    uint8_t blist[TSTRIDE];        // beneath triangles in index order / compaction map
+    uint8_t fstack[TSTRIDE];       // free triangle slots
+    uint16_t order[HMAX + 1];      // insertion order (slots)
+    float okey[HMAX + 1];
+    uint32_t bmask[TSTRIDE / 32];
+    uint32_t wasLink[HSLOTS / 32], insMask[HSLOTS / 32];
+    int nedge, nfree, ntri, nins, nhist, ncoord;
+};
+
+__device__ __forceinline__ double3 wpt(const WS& S, int slot) {
+    const int c = S.cix[slot];
+    return make_double3(S.cx[c], S.cy[c], S.cz[c]);
+}
+__device__ __forceinline__ int wid(const WS& S, int slot) { return S.hh[slot] & (int)HID; }
+
+__device__ __forceinline__ bool valid_id(const Dev& D, int v) { return (unsigned)v < (unsigned)D.n; }
+
+__device__ __forceinline__ PredSink sink_of(const Dev& D) {
+    PredSink k;
+    k.err = &D.ctr->err;
+    k.dbg_set = &D.ctr->dbg_set;
+    k.dbg_pts = D.ctr->dbg_pts;
+    k.dbg_ids = D.ctr->dbg_ids;
+    return k;
+}
+
+// point coordinates; an out-of-range id (only possible from a corrupted star)
+// raises ERR_TOPOLOGY and reads point 0 instead of leaving the buffer
+__device__ __forceinline__ double3 gpt(const Dev& D, int id) {
+    if (!valid_id(D, id)) {
+        atomicOr(&D.ctr->err, ERR_TOPOLOGY);
+        id = 0;
+    }
+    const double4 p = D.P[id];
+    return make_double3(p.x, p.y, p.z);
+}
+
+// cache the coordinates of the point in `slot`
+__device__ __forceinline__ void ws_cache_coords(WS& S, const Dev& D, int slot, int id) {
+    const int c = atomicAdd(&S.ncoord, 1);
+    const int cc = c < HMAX + 1 ? c : HMAX;
+    S.cix[slot] = (uint8_t)cc;
+    const double4 p = D.P[valid_id(D, id) ? id : 0];
+    S.cx[cc] = p.x;
+    S.cy[cc] = p.y;
+    S.cz[cc] = p.z;
+}
+
+// membership of v in star `star` (global hash): 0 = never inserted,
+// 1 = in the history but not in the link, 2 = in the link
+__device__ __forceinline__ int hist_state(const Dev& D, int star, int v) {
+    if (!valid_id(D, star)) return 1;  // never asks for an insertion into a bad star
+    const int* h = D.hh + (size_t)star * HSLOTS;
+    uint32_t s = hslot0(v);
+    for (int k = 0; k < HSLOTS; ++k) {
+        const uint32_t e = (uint32_t)h[s];
+        if ((e & HID) == (uint32_t)v) return (e & HLINK) ? 2 : 1;
+        if ((e & HID) == HEMPTY) return 0;
+        s = (s + 1) & (HSLOTS - 1);
+    }
+    return 0;
+}
+
+// slot of v in star's global hash, -1 if absent
+__device__ __forceinline__ int hist_slot(const Dev& D, int star, int v) {
+    const int* h = D.hh + (size_t)star * HSLOTS;
+    uint32_t s = hslot0(v);
+    for (int k = 0; k < HSLOTS; ++k) {
+        const uint32_t e = (uint32_t)h[s];
+        if ((e & HID) == (uint32_t)v) return (int)s;
+        if ((e & HID) == HEMPTY) return -1;
+        s = (s + 1) & (HSLOTS - 1);
+    }
+    return -1;
+}
+
+__device__ __forceinline__ void push_inbox(const Dev& D, int t, int v, bool* overflow) {
+    if (!valid_id(D, t) || !valid_id(D, v)) {
+        atomicOr(&D.ctr->err, ERR_TOPOLOGY);
+        return;
+    }
+    const int cnt = *((volatile int*)&D.inboxCount[t]);
+    const int* box = D.inbox + (size_t)t * INBOX_CAP;
+    const int lim = cnt < INBOX_CAP ? cnt : INBOX_CAP;
+    for (int k = 0; k < lim; ++k)
+        if (((volatile const int*)box)[k] == v) return;
+    const int pos = atomicAdd(&D.inboxCount[t], 1);
+    if (pos == 0) {
+        const int w = atomicAdd(&D.ctr->ins_count, 1);
+        D.wlIns[w] = t;
+    }
+    if (pos < INBOX_CAP)
+        D.inbox[(size_t)t * INBOX_CAP + pos] = v;
+    else
+        *overflow = true;
+}
+
+// --------------------------------------------------------------------------
+// warp helpers
+// --------------------------------------------------------------------------
+
+__device__ __forceinline__ int warp_excl_scan(int v, int lane, int* total) {
+    int incl = v;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off) incl += u;
+    }
+    *total = __shfl_sync(0xffffffffu, incl, 31);
+    return incl - v;
+}
+
+// Insert id v into the shared history hash; returns slot, sets *fresh when new.
+__device__ __forceinline__ int ws_hash_insert(WS& S, int v, bool* fresh) {
+    uint32_t s = hslot0(v);
+    for (int k = 0; k < HSLOTS; ++k) {
+        const int old = atomicCAS(&S.hh[s], (int)HEMPTY, v);
+        if ((uint32_t)old == HEMPTY) { *fresh = true; return (int)s; }
+        if ((old & (int)HID) == v) { *fresh = false; return (int)s; }
+        s = (s + 1) & (HSLOTS - 1);
+    }
+    *fresh = false;
+    return -1;
+}
+
+// Insert the point in slot sp into the star held by the warp. Returns 1 when it
+// entered the link, 0 when it lies inside the star's cone (drowned), -1 on an
+// error (flag raised).
+__device__ int warp_insert(WS& S, int lane, int s, double3 ps, int sp, int gen, const PredSink& sink,
+                           unsigned* exact) {
+    unsigned* err = sink.err;
+    const double3 pp = wpt(S, sp);
+    const int pid = wid(S, sp);
+    const int ntri = S.ntri;
+    int nb = 0, nalive = 0;
+    for (int base = 0; base < ntri; base += 32) {
+        const int t = base + lane;
+        bool b = false, al = false;
+        if (t < ntri && (S.tf[t] & 0x80)) {
+            al = true;
+            const int a = S.tv[0][t], bb = S.tv[1][t], c = S.tv[2][t];
+            b = orient4(wpt(S, a), wpt(S, bb), wpt(S, c), ps, pp, wid(S, a), wid(S, bb), wid(S, c), s, pid, sink,
+                        exact) < 0;
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, b);
+        nalive += __popc(__ballot_sync(0xffffffffu, al));
+        if (lane == 0) S.bmask[base >> 5] = m;
+        nb += __popc(m);
+    }
+    __syncwarp();
+    if (nb == 0) return 0;
+    if (nb == nalive) {
+        if (lane == 0) {
+            atomicOr(err, ERR_TOPOLOGY);
+            G4D_TRACE("star %d: point %d beneath all %d triangles\n", s, pid, nalive);
+        }
+        return -1;
+    }
+    // beneath triangles in index order, and the hole's boundary edges
+    int nedge = 0, prefix = 0;
+    for (int base = 0; base < ntri; base += 32) {
+        const unsigned m = S.bmask[base >> 5];
+        const int t = base + lane;
+        const bool b = (m >> lane) & 1u;
+        if (b) S.blist[prefix + __popc(m & ((1u << lane) - 1u))] = (uint8_t)t;
+        prefix += __popc(m);
+        uint32_t rec[3];
+        int ne = 0;
+        if (b) {
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const int o = S.to[i][t];
+                const bool ob = (S.bmask[o >> 5] >> (o & 31)) & 1u;
+                if (!ob) {
+                    const int u = S.tv[(i + 1) % 3][t], w = S.tv[(i + 2) % 3][t];
+                    rec[ne++] = (uint32_t)u | ((uint32_t)w << 9) | ((uint32_t)o << 18) | ((uint32_t)S.tj[i][t] << 26);
+                }
+            }
+        }
+        int total;
+        const int start = nedge + warp_excl_scan(ne, lane, &total);
+        for (int k = 0; k < ne; ++k)
+            if (start + k < TSTRIDE) S.erec[start + k] = rec[k];
+        nedge += total;
+    }
+    __syncwarp();
+    const int B = nedge;
+    if (B > HMAX) {  // a disk's boundary visits each link vertex at most once
+        if (lane == 0) {
+            atomicOr(err, ERR_TOPOLOGY);
+            G4D_TRACE("star %d: point %d hole boundary of %d edges\n", s, pid, B);
+        }
+        return -1;
+    }
+    const int nfree = S.nfree;
+    // the B new triangles reuse the nb holes first, then free slots, then append
+    const int extra = B - nb;
+    const int from_free = extra > 0 ? (extra < nfree ? extra : nfree) : 0;
+    const int appended = extra > 0 ? extra - from_free : 0;
+    if (ntri + appended > TMAX) {
+        if (lane == 0) {
+            atomicOr(err, ERR_CAPACITY);
+            G4D_TRACE("star %d: point %d needs %d triangles (nb %d, B %d, free %d)\n", s, pid, ntri + appended, nb,
+                      B, nfree);
+        }
+        return -1;
+    }
+    for (int r = lane; r < B; r += 32) {
+        const uint32_t e = S.erec[r];
+        const int u = e & 511, w = (e >> 9) & 511;
+        int slot;
+        if (r < nb) {
+            slot = S.blist[r];
+        } else {
+            const int rr = r - nb;
+            slot = rr < nfree ? S.fstack[nfree - 1 - rr] : ntri + (rr - nfree);
+        }
+        S.efrom[u] = (uint8_t)slot;
+        S.eto[w] = (uint8_t)slot;
+    }
+    __syncwarp();
+    // new triangle (u, w, p) replaces the beneath triangle across the edge u->w
+    for (int r = lane; r < B; r += 32) {
+        const uint32_t e = S.erec[r];
+        const int u = e & 511, w = (e >> 9) & 511, o = (e >> 18) & 255, oj = (e >> 26) & 3;
+        const int slot = S.efrom[u];
+        S.tv[0][slot] = (uint16_t)u;
+        S.tv[1][slot] = (uint16_t)w;
+        S.tv[2][slot] = (uint16_t)sp;
+        S.to[0][slot] = S.efrom[w];  // edge (w, p): the next boundary edge's triangle
+        S.tj[0][slot] = 1;
+        S.to[1][slot] = S.eto[u];    // edge (p, u): the previous boundary edge's triangle
+        S.tj[1][slot] = 0;
+        S.to[2][slot] = (uint8_t)o;  // edge (u, w): the triangle outside the hole
+        S.tj[2][slot] = (uint8_t)oj;
+        if (oj < 3) {
+            S.to[oj][o] = (uint8_t)slot;
+            S.tj[oj][o] = 2;
+        }
+        S.tf[slot] = (uint8_t)(0x80 | gen);
+    }
+    __syncwarp();
+    if (B < nb) {
+        for (int r = B + lane; r < nb; r += 32) {
+            const int t = S.blist[r];
+            S.tf[t] = 0;
+            S.fstack[nfree + (r - B)] = (uint8_t)t;
+        }
+    }
+    __syncwarp();
+    if (lane == 0) {
+        if (B < nb) {
+            S.nfree = nfree + (nb - B);
+        } else {
+            S.nfree = nfree - from_free;
+            S.ntri = ntri + appended;
+        }
+    }
+    __syncwarp();
+    return 1;
+}
+
+// cone of the pentachoron (l0..l3, star): the link triangles of the 4-simplex
+// (GDelPredKernels.cu:45-158), oriented so that orient4(tri, star, opposite) > 0
+__device__ void warp_cone(WS& S, int lane, int s, double3 ps, const int* l4, int gen, const PredSink& sink,
+                          unsigned* exact) {
+    int l[4] = {l4[0], l4[1], l4[2], l4[3]};
+    const int o = orient4(wpt(S, l[0]), wpt(S, l[1]), wpt(S, l[2]), wpt(S, l[3]), ps, wid(S, l[0]), wid(S, l[1]),
+                          wid(S, l[2]), wid(S, l[3]), s, sink, exact);
+    if (o < 0) { const int t = l[0]; l[0] = l[1]; l[1] = t; }
+    if (lane < 4) {
+        const int F[4][3] = {{1, 2, 3}, {0, 3, 2}, {0, 1, 3}, {0, 2, 1}};
+        const int f = lane;
+        for (int i = 0; i < 3; ++i) {
+            S.tv[i][f] = (uint16_t)l[F[f][i]];
+            const int b = F[f][i];  // the face omitting vertex F[f][i] shares this edge
+            S.to[i][f] = (uint8_t)b;
+            int j = 0;
+            for (int k = 0; k < 3; ++k)
+                if (F[b][k] == f) j = k;
+            S.tj[i][f] = (uint8_t)j;
+        }
+        S.tf[f] = (uint8_t)(0x80 | gen);
+    }
+    if (lane == 0) {
+        S.ntri = 4;
+        S.nfree = 0;
+    }
+    __syncwarp();
+}
+
+// sort order[0..n) by okey ascending (bitonic over a power of two <= HMAX + 1)
+__device__ void warp_sort_order(WS& S, int lane, int n) {
+    int m = 1;
+    while (m < n) m <<= 1;
+    for (int i = n + lane; i < m; i += 32) { S.okey[i] = 3.0e38f; S.order[i] = 0; }
+    __syncwarp();
+    for (int k = 2; k <= m; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = lane; i < m; i += 32) {
+                const int p = i ^ j;
+                if (p > i) {
+                    const bool up = (i & k) == 0;
+                    const float a = S.okey[i], b = S.okey[p];
+                    if ((a > b) == up) {
+                        S.okey[i] = b; S.okey[p] = a;
+                        const uint16_t t = S.order[i]; S.order[i] = S.order[p]; S.order[p] = t;
+                    }
+                }
+            }
+            __syncwarp();
+        }
+}
+
+// Load star s (history, coordinates, triangles) into shared memory.
+__device__ void warp_load(WS& S, const Dev& D, int lane, int s, StarHdr h) {
+    if (lane == 0) {
+        S.ncoord = 0;
+        S.nins = 0;
+    }
+    __syncwarp();
+    const int* gh = D.hh + (size_t)s * HSLOTS;
+    for (int k = lane; k < HSLOTS; k += 32) {
+        const int e = gh[k];
+        S.hh[k] = e;
+        const bool occ = (uint32_t)(e & (int)HID) != HEMPTY;
+        if (occ) ws_cache_coords(S, D, k, e & (int)HID);
+        const unsigned m = __ballot_sync(0xffffffffu, occ && (e & (int)HLINK) != 0);
+        if (lane == 0) { S.wasLink[k >> 5] = m; S.insMask[k >> 5] = 0; }
+    }
+    const uint2* gt = D.tri + (size_t)s * TSTRIDE;
+    for (int t = lane; t < h.ntri; t += 32) {
+        const uint2 T = gt[t];
+        S.tv[0][t] = (uint16_t)tri_v(T, 0);
+        S.tv[1][t] = (uint16_t)tri_v(T, 1);
+        S.tv[2][t] = (uint16_t)tri_v(T, 2);
+        S.tf[t] = (uint8_t)(0x80 | tri_gen(T));
+        S.to[0][t] = (uint8_t)tri_o(T, 0); S.to[1][t] = (uint8_t)tri_o(T, 1); S.to[2][t] = (uint8_t)tri_o(T, 2);
+        S.tj[0][t] = (uint8_t)tri_j(T, 0); S.tj[1][t] = (uint8_t)tri_j(T, 1); S.tj[2][t] = (uint8_t)tri_j(T, 2);
+    }
+    if (lane == 0) {
+        S.ntri = h.ntri;
+        S.nhist = h.nhist;
+        S.nfree = 0;
+    }
+    __syncwarp();
+}
+
+// Compact triangles, refresh link bits, report drowned points, write back.
+__device__ void warp_store(WS& S, const Dev& D, int lane, int s, int pass, bool created) {
+    const int ntri = S.ntri;
+    int nalive = 0;
+    // new index of each live triangle (blist reused as the map)
+    for (int base = 0; base < ntri; base += 32) {
+        const int t = base + lane;
+        const bool al = t < ntri && (S.tf[t] & 0x80);
+        const unsigned m = __ballot_sync(0xffffffffu, al);
+        if (al) S.blist[t] = (uint8_t)(nalive + __popc(m & ((1u << lane) - 1u)));
+        nalive += __popc(m);
+    }
+    for (int k = lane; k < HSLOTS; k += 32) S.hh[k] &= (int)HID;
+    __syncwarp();
+    for (int t = lane; t < ntri; t += 32) {
+        if (!(S.tf[t] & 0x80)) continue;
+        for (int i = 0; i < 3; ++i) atomicOr(&S.hh[S.tv[i][t]], (int)HLINK);
+    }
+    __syncwarp();
+    uint2* gt = D.tri + (size_t)s * TSTRIDE;
+    for (int t = lane; t < ntri; t += 32) {
+        if (!(S.tf[t] & 0x80)) continue;
+        gt[S.blist[t]] = tri_pack(S.tv[0][t], S.tv[1][t], S.tv[2][t], S.tf[t] & 15, S.blist[S.to[0][t]],
+                                  S.blist[S.to[1][t]], S.blist[S.to[2][t]], S.tj[0][t], S.tj[1][t], S.tj[2][t]);
+    }
+    // drowned: linked before or inserted now, not linked after
+    int* gh = D.hh + (size_t)s * HSLOTS;
+    for (int k = lane; k < HSLOTS; k += 32) {
+        const int e = S.hh[k];
+        gh[k] = e;
+        const bool occupied = (uint32_t)(e & (int)HID) != HEMPTY;
+        const bool before = ((S.wasLink[k >> 5] | S.insMask[k >> 5]) >> (k & 31)) & 1u;
+        const bool dr = occupied && before && !(e & (int)HLINK);
+        const unsigned m = __ballot_sync(0xffffffffu, dr);
+        if (m) {
+            int base = 0;
+            if (lane == 0) base = atomicAdd(&D.ctr->drown_next, __popc(m));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (dr) {
+                const int pos = base + __popc(m & ((1u << lane) - 1u));
+                if (pos < D.drownCap) D.drownNext[pos] = make_int2(s, e & (int)HID);
+                else atomicOr(&D.ctr->err, ERR_DROWNCAP);
+            }
+        }
+    }
+    if (lane == 0) {
+        StarHdr h;
+        h.ntri = (uint8_t)nalive;
+        h.nhist = (uint8_t)S.nhist;
+        h.pass = (uint8_t)pass;
+        h.flags = HDR_BUILT;
+        D.hdr[s] = h;
+        if (created) {
+            const int w = atomicAdd(&D.ctr->emit_next, 1);
+            D.wlEmitNext[w] = s;
+        }
+    }
+    __syncwarp();
+}
+
+// --------------------------------------------------------------------------
+// build: initial star of every point from its candidate workset
+// --------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_star_build(Dev D) {
+    G4D_DYN_SMEM(smem_raw);
+    const int lane = threadIdx.x & 31;
+    WS& S = reinterpret_cast<WS*>(smem_raw)[threadIdx.x >> 5];
+    const PredSink sink = sink_of(D);
+    unsigned* err = sink.err;
+    unsigned* exact = &D.ctr->exact;
+    const int warps = gridDim.x * WARPS_PER_BLOCK;
+    for (int s = blockIdx.x * WARPS_PER_BLOCK + (threadIdx.x >> 5); s < D.n; s += warps) {
+        __syncwarp();  // the previous star's shared-memory reads are done
+        for (int k = lane; k < HSLOTS; k += 32) S.hh[k] = (int)HEMPTY;
+        for (int k = lane; k < HSLOTS / 32; k += 32) { S.wasLink[k] = 0; S.insMask[k] = 0; }
+        if (lane == 0) { S.nins = 0; S.nhist = 0; S.ntri = 0; S.nfree = 0; S.ncoord = 0; }
+        __syncwarp();
+        const double3 ps = gpt(D, s);
+        // candidates from the bucket
+        const int bc = min(D.bucketCount[s], BUCKET_CAP);
+        for (int k = lane; k < bc; k += 32) {
+            const int v = D.bucket[(size_t)s * BUCKET_CAP + k];
+            if (v == s || !valid_id(D, v)) continue;
+            bool fresh;
+            const int slot = ws_hash_insert(S, v, &fresh);
+            if (fresh) {
+                const int pos = atomicAdd(&S.nins, 1);
+                S.order[pos] = (uint16_t)slot;
+            }
+        }
+        __syncwarp();
+        const int ncand = S.nins;
+        __syncwarp();  // every lane has read the count before lane 0 may change it
+        // pumping (GDelKernels.cu:370-477): fewer than MIN_WORKSET candidates borrow
+        // from their candidates' worksets, then from the first point ids
+        if (ncand < MIN_WORKSET) {
+            if (lane == 0) {
+                int have = ncand;
+                for (int i = 0; i < ncand && have < MIN_WORKSET; ++i) {
+                    const int c = S.hh[S.order[i]] & (int)HID;
+                    const int cc = min(D.bucketCount[c], BUCKET_CAP);
+                    for (int k = 0; k < cc && have < MIN_WORKSET; ++k) {
+                        const int v = D.bucket[(size_t)c * BUCKET_CAP + k];
+                        if (v == s || !valid_id(D, v)) continue;
+                        bool fresh;
+                        const int slot = ws_hash_insert(S, v, &fresh);
+                        if (fresh) S.order[have++] = (uint16_t)slot;
+                    }
+                }
+                for (int v = 0; v < D.n && have < MIN_WORKSET; ++v) {
+                    if (v == s) continue;
+                    bool fresh;
+                    const int slot = ws_hash_insert(S, v, &fresh);
+                    if (fresh) S.order[have++] = (uint16_t)slot;
+                }
+                // reciprocal requests for the pumped points
+                bool ovf = false;
+                for (int i = ncand; i < have; ++i) push_inbox(D, S.hh[S.order[i]] & (int)HID, s, &ovf);
+                if (ovf) atomicOr(&D.ctr->overflow, 1);
+                S.nins = have;
+            }
+            __syncwarp();
+        }
+        const int nins = S.nins;
+        if (nins > HMAX || nins < 4) {
+            if (lane == 0) {
+                atomicOr(err, nins > HMAX ? ERR_CAPACITY : ERR_TOPOLOGY);
+                G4D_TRACE("star %d: %d initial candidates\n", s, nins);
+            }
+            continue;
+        }
+        // coordinates, distances, insertion order (nearest first)
+        for (int i = lane; i < nins; i += 32) {
+            const int slot = S.order[i];
+            const int id = S.hh[slot] & (int)HID;
+            ws_cache_coords(S, D, slot, id);
+            const double3 p = wpt(S, slot);
+            const double dx = p.x - ps.x, dy = p.y - ps.y, dz = p.z - ps.z;
+            S.okey[i] = (float)(dx * dx + dy * dy + dz * dz);
+            atomicOr(&S.insMask[slot >> 5], 1u << (slot & 31));
+        }
+        __syncwarp();
+        warp_sort_order(S, lane, nins);
+        if (lane == 0) S.nhist = nins;
+        __syncwarp();
+        const int gen = 1;
+        int l4[4] = {S.order[0], S.order[1], S.order[2], S.order[3]};
+        warp_cone(S, lane, s, ps, l4, gen, sink, exact);
+        int failed = 0;
+        for (int i = 4; i < nins && !failed; ++i) {
+            const int r = warp_insert(S, lane, s, ps, S.order[i], gen, sink, exact);
+            failed = r < 0;
+        }
+        if (failed) continue;
+        warp_store(S, D, lane, s, gen, true);
+        if (lane == 0) atomicAdd(&D.ctr->insertions, (unsigned long long)nins);
+    }
+}
+
+// --------------------------------------------------------------------------
+// insertion round: every star with inbox requests
+// --------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_star_insert(Dev D, int count) {
+    G4D_DYN_SMEM(smem_raw);
+    const int lane = threadIdx.x & 31;
+    WS& S = reinterpret_cast<WS*>(smem_raw)[threadIdx.x >> 5];
+    const PredSink sink = sink_of(D);
+    unsigned* err = sink.err;
+    unsigned* exact = &D.ctr->exact;
+    const int warps = gridDim.x * WARPS_PER_BLOCK;
+    for (int w = blockIdx.x * WARPS_PER_BLOCK + (threadIdx.x >> 5); w < count; w += warps) {
+        __syncwarp();  // the previous item's shared-memory reads are done
+        const int s = D.wlIns[w];
+        const StarHdr h = D.hdr[s];
+        warp_load(S, D, lane, s, h);
+        const double3 ps = gpt(D, s);
+        const int ic = min(D.inboxCount[s], INBOX_CAP);
+        int* box = D.inbox + (size_t)s * INBOX_CAP;
+        for (int k = lane; k < ic; k += 32) {
+            const int v = box[k];
+            box[k] = -1;
+            if (v == s || !valid_id(D, v)) continue;
+            bool fresh;
+            const int slot = ws_hash_insert(S, v, &fresh);
+            if (slot < 0) { atomicOr(err, ERR_CAPACITY); continue; }
+            if (fresh) {
+                const int pos = atomicAdd(&S.nins, 1);
+                S.order[pos < HMAX ? pos : HMAX] = (uint16_t)slot;
+                ws_cache_coords(S, D, slot, v);
+                atomicOr(&S.insMask[slot >> 5], 1u << (slot & 31));
+            }
+        }
+        __syncwarp();
+        if (lane == 0) D.inboxCount[s] = 0;
+        const int nins = S.nins;
+        const int nhist0 = S.nhist;
+        __syncwarp();  // all lanes read the counts before lane 0 updates them
+        if (nhist0 + nins > HMAX) {
+            if (lane == 0) {
+                atomicOr(err, ERR_CAPACITY);
+                G4D_TRACE("star %d: history %d + %d exceeds %d\n", s, nhist0, nins, HMAX);
+            }
+            continue;
+        }
+        if (lane == 0) S.nhist = nhist0 + nins;
+        __syncwarp();
+        const int gen = (h.pass % 15) + 1;  // 1..15, differs from the stored pass
+        int any = 0, failed = 0;
+        for (int i = 0; i < nins && !failed; ++i) {
+            const int r = warp_insert(S, lane, s, ps, S.order[i], gen, sink, exact);
+            failed = r < 0;
+            any |= r > 0;
+        }
+        if (failed) continue;
+        warp_store(S, D, lane, s, any ? gen : h.pass, any != 0);
+        if (lane == 0) atomicAdd(&D.ctr->insertions, (unsigned long long)nins);
+    }
+}
+
+// --------------------------------------------------------------------------
+// emission: every link edge (u,v) of a fresh triangle asks that u and v know
+// each other (GDelKernels.cu:818-939)
+// --------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_emit(Dev D, int count) {
+    __shared__ int shh[WARPS_PER_BLOCK][HSLOTS];
+    const int lane = threadIdx.x & 31;
+    int* hh = shh[threadIdx.x >> 5];
+    const int warps = gridDim.x * WARPS_PER_BLOCK;
+    for (int w = blockIdx.x * WARPS_PER_BLOCK + (threadIdx.x >> 5); w < count; w += warps) {
+        __syncwarp();  // the previous item's shared-memory reads are done
+        const int s = D.wlEmit[w];
+        StarHdr h = D.hdr[s];
+        const bool all = (h.flags & HDR_EMIT_ALL) != 0;
+        const int* gh = D.hh + (size_t)s * HSLOTS;
+        for (int k = lane; k < HSLOTS; k += 32) hh[k] = gh[k] & (int)HID;
+        __syncwarp();
+        const uint2* gt = D.tri + (size_t)s * TSTRIDE;
+        bool ovf = false;
+        for (int t = lane; t < h.ntri; t += 32) {
+            const uint2 T = gt[t];
+            if (!all && tri_gen(T) != h.pass) continue;
+            const int v[3] = {hh[tri_v(T, 0)], hh[tri_v(T, 1)], hh[tri_v(T, 2)]};
+            for (int i = 0; i < 3; ++i) {
+                const int a = v[i], b = v[(i + 1) % 3];
+                if (a > b) continue;
+                if (!valid_id(D, a) || !valid_id(D, b)) {
+                    atomicOr(&D.ctr->err, ERR_TOPOLOGY);
+                    continue;
+                }
+                if (hist_state(D, a, b) == 0) push_inbox(D, a, b, &ovf);
+                if (hist_state(D, b, a) == 0) push_inbox(D, b, a, &ovf);
+            }
+        }
+        const unsigned anyovf = __ballot_sync(0xffffffffu, ovf);
+        if (lane == 0) {
+            if (anyovf) {
+                h.flags |= HDR_EMIT_ALL;
+                const int q = atomicAdd(&D.ctr->emit_next, 1);
+                D.wlEmitNext[q] = s;
+                atomicOr(&D.ctr->overflow, 1);
+            } else {
+                h.flags &= ~HDR_EMIT_ALL;
+            }
+            D.hdr[s] = h;
+        }
+        __syncwarp();
+    }
+}
+
+// --------------------------------------------------------------------------
+// containment proofs for drowned points (GDelPredKernels.cu:427-626)
+// --------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_proof(Dev D, int count) {
+    __shared__ int shh[WARPS_PER_BLOCK][HSLOTS];
+    const int lane = threadIdx.x & 31;
+    int* hh = shh[threadIdx.x >> 5];
+    const PredSink sink = sink_of(D);
+    unsigned* err = sink.err;
+    unsigned* exact = &D.ctr->exact;
+    const int warps = gridDim.x * WARPS_PER_BLOCK;
+    for (int w = blockIdx.x * WARPS_PER_BLOCK + (threadIdx.x >> 5); w < count; w += warps) {
+        __syncwarp();  // the previous item's shared-memory reads are done
+        const int2 item = D.drown[w];
+        const int s = item.x, v = item.y;
+        if (!valid_id(D, s) || !valid_id(D, v)) continue;
+        // a proof is needed only while v's star still links back to s
+        if (hist_state(D, v, s) != 2) continue;
+        const StarHdr h = D.hdr[s];
+        if (h.ntri == 0) continue;
+        const int* gh = D.hh + (size_t)s * HSLOTS;
+        for (int k = lane; k < HSLOTS; k += 32) hh[k] = gh[k] & (int)HID;
+        __syncwarp();
+        const uint2* gt = D.tri + (size_t)s * TSTRIDE;
+        const double3 ps = gpt(D, s), pv = gpt(D, v);
+        const int ex = hh[tri_v(gt[0], 0)];
+        const double3 pe = gpt(D, ex);
+        int found_t = 0x7fffffff;
+        int pa = -1, pb = -1, pc = -1;
+        for (int base = 0; base < h.ntri; base += 32) {
+            const int t = base + lane;
+            bool ok = false;
+            int a = -1, b = -1, c = -1;
+            if (t < h.ntri) {
+                const uint2 T = gt[t];
+                a = hh[tri_v(T, 0)]; b = hh[tri_v(T, 1)]; c = hh[tri_v(T, 2)];
+                if (a != ex && b != ex && c != ex) {
+                    const double3 qa = gpt(D, a), qb = gpt(D, b), qc = gpt(D, c);
+                    const int o0 = orient4(ps, pv, pe, qa, qb, s, v, ex, a, b, sink, exact);
+                    const int o1 = orient4(ps, pv, pe, qb, qc, s, v, ex, b, c, sink, exact);
+                    ok = o0 == o1;
+                    if (ok) {
+                        const int o2 = orient4(ps, pv, pe, qc, qa, s, v, ex, c, a, sink, exact);
+                        ok = o1 == o2;
+                    }
+                }
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, ok);
+            if (m) {
+                const int src = __ffs(m) - 1;
+                found_t = base + src;
+                pa = __shfl_sync(0xffffffffu, a, src);
+                pb = __shfl_sync(0xffffffffu, b, src);
+                pc = __shfl_sync(0xffffffffu, c, src);
+                break;
+            }
+        }
+        if (found_t == 0x7fffffff) {
+            if (lane == 0) {
+                atomicOr(err, ERR_PROOF);
+                G4D_TRACE("star %d: no containment proof for %d\n", s, v);
+            }
+            continue;
+        }
+        bool ovf = false;
+        if (lane < 4) {
+            const int q = lane == 0 ? ex : (lane == 1 ? pa : (lane == 2 ? pb : pc));
+            if (q != v) {
+                if (hist_state(D, v, q) == 0) push_inbox(D, v, q, &ovf);
+                if (hist_state(D, q, v) == 0) push_inbox(D, q, v, &ovf);
+            }
+        }
+        const unsigned anyovf = __ballot_sync(0xffffffffu, ovf);
+        if (lane == 0) {
+            atomicAdd(&D.ctr->proofs_total, 1ull);
+            if (anyovf) {
+                const int q = atomicAdd(&D.ctr->drown_next, 1);
+                if (q < D.drownCap) D.drownNext[q] = item;
+                atomicOr(&D.ctr->overflow, 1);
+            }
+        }
+    }
+}
+
+// --------------------------------------------------------------------------
+// consistency check (GDelKernels.cu:1193-1271): triangle (a,b,c) of star s must
+// appear as the cyclic triangle (b,s,c) in star a
+// --------------------------------------------------------------------------
+
+// index of the triangle of `star` with vertex ids {x,y,z} (cyclic x,y,z when
+// `cyclic`), or -1
+__device__ int find_tri(const Dev& D, int star, int x, int y, int z, bool cyclic) {
+    if (!valid_id(D, star)) return -1;
+    const int sx = hist_slot(D, star, x), sy = hist_slot(D, star, y), sz = hist_slot(D, star, z);
+    if (sx < 0 || sy < 0 || sz < 0) return -1;
+    const StarHdr hd = D.hdr[star];
+    const uint2* gt = D.tri + (size_t)star * TSTRIDE;
+    for (int t = 0; t < hd.ntri; ++t) {
+        const uint2 T = gt[t];
+        const int a = tri_v(T, 0), b = tri_v(T, 1), c = tri_v(T, 2);
+        if (cyclic) {
+            if ((a == sx && b == sy && c == sz) || (b == sx && c == sy && a == sz) || (c == sx && a == sy && b == sz))
+                return t;
+        } else {
+            const bool hx = a == sx || b == sx || c == sx, hy = a == sy || b == sy || c == sy,
+                       hz = a == sz || b == sz || c == sz;
+            if (hx && hy && hz) return t;
+        }
+    }
+    return -1;
+}
+
+__global__ void k_check(Dev D, unsigned long long* bad) {
+    const int lane = threadIdx.x & 31;
+    const int warps = gridDim.x * (blockDim.x >> 5);
+    unsigned long long cnt = 0;
+    for (int s = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); s < D.n; s += warps) {
+        const StarHdr h = D.hdr[s];
+        const int* gh = D.hh + (size_t)s * HSLOTS;
+        const uint2* gt = D.tri + (size_t)s * TSTRIDE;
+        for (int t = lane; t < h.ntri; t += 32) {
+            const uint2 T = gt[t];
+            const int v[3] = {gh[tri_v(T, 0)] & (int)HID, gh[tri_v(T, 1)] & (int)HID, gh[tri_v(T, 2)] & (int)HID};
+            for (int i = 0; i < 3; ++i)
+                if (find_tri(D, v[i], v[(i + 1) % 3], s, v[(i + 2) % 3], true) < 0) ++cnt;
+        }
+    }
+    for (int o = 16; o; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    if (lane == 0 && cnt) atomicAdd(bad, cnt);
+}
+
+// --------------------------------------------------------------------------
+// extraction (GDelHost.cu:1520-1607): owner triangle (star < its 3 vertices) on
+// the lower hull, orient3d(v0,v1,v2,star) < 0, is a Delaunay tetrahedron
+// --------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_tet_count(Dev D, int* cnt) {
+    __shared__ int shh[WARPS_PER_BLOCK][HSLOTS];
+    const int lane = threadIdx.x & 31;
+    int* hh = shh[threadIdx.x >> 5];
+    const PredSink sink = sink_of(D);
+    const int warps = gridDim.x * WARPS_PER_BLOCK;
+    for (int s = blockIdx.x * WARPS_PER_BLOCK + (threadIdx.x >> 5); s < D.n; s += warps) {
+        __syncwarp();  // the previous star's shared-memory reads are done
+        const StarHdr h = D.hdr[s];
+        const int* gh = D.hh + (size_t)s * HSLOTS;
+        for (int k = lane; k < HSLOTS; k += 32) hh[k] = gh[k] & (int)HID;
+        __syncwarp();
+        uint2* gt = D.tri + (size_t)s * TSTRIDE;
+        const double3 ps = gpt(D, s);
+        int c = 0;
+        for (int t = lane; t < h.ntri; t += 32) {
+            const uint2 T = gt[t];
+            const int a = hh[tri_v(T, 0)], b = hh[tri_v(T, 1)], cc = hh[tri_v(T, 2)];
+            bool keep = false;
+            if (s < a && s < b && s < cc) keep = orient3d(gpt(D, a), gpt(D, b), gpt(D, cc), ps, sink) < 0;
+            const uint32_t nx = keep ? (T.x | TRI_KEPT) : (T.x & ~TRI_KEPT);
+            if (nx != T.x) gt[t].x = nx;
+            c += keep;
+        }
+        for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+        if (lane == 0) cnt[s] = c;
+    }
+}
+
+// tet id of the kept tetrahedron owned by `star` (its smallest vertex) whose
+// other vertices are {x,y,z}, or -1
+__device__ int owned_tet_id(const Dev& D, const int* base, int star, int x, int y, int z) {
+    const int ti = find_tri(D, star, x, y, z, false);
+    if (ti < 0) return -1;
+    const uint2* gt = D.tri + (size_t)star * TSTRIDE;
+    if (!(gt[ti].x & TRI_KEPT)) return -1;
+    int r = 0;
+    for (int t = 0; t < ti; ++t) r += (int)(gt[t].x >> 31);
+    return base[star] + r;
+}
+
+__global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_tet_write(Dev D, const int* base, g4d_tet* tets,
+                                                                    const int* sorted_to_input) {
+    __shared__ int shh[WARPS_PER_BLOCK][HSLOTS];
+    __shared__ uint8_t srank[WARPS_PER_BLOCK][TSTRIDE];
+    const int lane = threadIdx.x & 31;
+    int* hh = shh[threadIdx.x >> 5];
+    uint8_t* rank = srank[threadIdx.x >> 5];
+    const int warps = gridDim.x * WARPS_PER_BLOCK;
+    for (int s = blockIdx.x * WARPS_PER_BLOCK + (threadIdx.x >> 5); s < D.n; s += warps) {
+        __syncwarp();  // the previous star's shared-memory reads are done
+        const StarHdr h = D.hdr[s];
+        const int* gh = D.hh + (size_t)s * HSLOTS;
+        for (int k = lane; k < HSLOTS; k += 32) hh[k] = gh[k] & (int)HID;
+        const uint2* gt = D.tri + (size_t)s * TSTRIDE;
+        int pre = 0;
+        for (int b0 = 0; b0 < h.ntri; b0 += 32) {
+            const int t = b0 + lane;
+            const bool kept = t < h.ntri && (gt[t].x & TRI_KEPT);
+            const unsigned m = __ballot_sync(0xffffffffu, kept);
+            if (t < h.ntri) rank[t] = (uint8_t)(pre + __popc(m & ((1u << lane) - 1u)));
+            pre += __popc(m);
+        }
+        __syncwarp();
+        for (int t = lane; t < h.ntri; t += 32) {
+            const uint2 T = gt[t];
+            if (!(T.x & TRI_KEPT)) continue;
+            const int sl[3] = {tri_v(T, 0), tri_v(T, 1), tri_v(T, 2)};
+            const int v[3] = {hh[sl[0]], hh[sl[1]], hh[sl[2]]};
+            g4d_tet out;
+            // neighbours across the faces that contain s: adjacent link triangles
+            for (int i = 0; i < 3; ++i) {
+                const int oi = tri_o(T, i);
+                const uint2 N = gt[oi];
+                const int e1 = sl[(i + 1) % 3], e2 = sl[(i + 2) % 3];
+                int xs = tri_v(N, 0);
+                for (int k = 0; k < 3; ++k)
+                    if (tri_v(N, k) != e1 && tri_v(N, k) != e2) xs = tri_v(N, k);
+                const int x = hh[xs];
+                if (x > s)
+                    out.opp[i] = (N.x & TRI_KEPT) ? base[s] + rank[oi] : -1;
+                else
+                    out.opp[i] = owned_tet_id(D, base, x, s, v[(i + 1) % 3], v[(i + 2) % 3]);
+            }
+            // neighbour across the face (v0, v1, v2): through star v0
+            {
+                int res = -1;
+                const int a = v[0], b = v[1], c = v[2];
+                const int ta = find_tri(D, a, b, s, c, false);
+                if (ta >= 0) {
+                    const int* ah = D.hh + (size_t)a * HSLOTS;
+                    const uint2* at = D.tri + (size_t)a * TSTRIDE;
+                    const uint2 A = at[ta];
+                    int pos = 0;
+                    for (int k = 0; k < 3; ++k)
+                        if ((ah[tri_v(A, k)] & (int)HID) == s) pos = k;
+                    const uint2 N = at[tri_o(A, pos)];
+                    int y = -1;
+                    for (int k = 0; k < 3; ++k) {
+                        const int id = ah[tri_v(N, k)] & (int)HID;
+                        if (id != b && id != c) y = id;
+                    }
+                    if (y >= 0) {
+                        const int all4[4] = {a, b, c, y};
+                        int m = a;
+                        for (int k = 1; k < 4; ++k) m = all4[k] < m ? all4[k] : m;
+                        int q[3], nq = 0;
+                        for (int k = 0; k < 4; ++k)
+                            if (all4[k] != m && nq < 3) q[nq++] = all4[k];
+                        if (nq == 3) res = owned_tet_id(D, base, m, q[0], q[1], q[2]);
+                    }
+                }
+                out.opp[3] = res;
+            }
+            if (sorted_to_input) {
+                out.v[0] = sorted_to_input[v[0]];
+                out.v[1] = sorted_to_input[v[1]];
+                out.v[2] = sorted_to_input[v[2]];
+                out.v[3] = sorted_to_input[s];
+            } else {
+                out.v[0] = v[0]; out.v[1] = v[1]; out.v[2] = v[2]; out.v[3] = s;
+            }
+            tets[base[s] + rank[t]] = out;
+        }
+    }
+}
+
+#ifndef G4D_HOST_EMULATION
+// --------------------------------------------------------------------------
+// diagnostic predicate evaluation
+// --------------------------------------------------------------------------
+
+__global__ void k_eval_pred(int kind, const double* pts, const int* idx, int count, int8_t* out, unsigned* errw) {
+    PredSink err;
+    err.err = errw;
+    err.dbg_set = nullptr;
+    err.dbg_pts = nullptr;
+    err.dbg_ids = nullptr;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        if (kind == 0) {
+            const double* p = pts + 12 * (size_t)i;
+            out[i] = (int8_t)orient3d(make_double3(p[0], p[1], p[2]), make_double3(p[3], p[4], p[5]),
+                                      make_double3(p[6], p[7], p[8]), make_double3(p[9], p[10], p[11]), err);
+        } else {
+            const double* p = pts + 15 * (size_t)i;
+            double3 q[5];
+            for (int k = 0; k < 5; ++k) q[k] = make_double3(p[3 * k], p[3 * k + 1], p[3 * k + 2]);
+            if (kind == 1) {
+                const int* id = idx + 5 * (size_t)i;
+                out[i] = (int8_t)orient4(q[0], q[1], q[2], q[3], q[4], id[0], id[1], id[2], id[3], id[4], err,
+                                         nullptr);
+            } else {
+                int f = orient4_filter(q[0], q[1], q[2], q[3], q[4]);
+                if (!f) {
+                    IntPts<2> P;
+                    if (to_int_points<2>(q, 5, P)) f = orient4_int<2>(P);
+                    else {
+                        IntPts<4> P4;
+                        if (to_int_points<4>(q, 5, P4)) f = orient4_int<4>(P4);
+                        else atomicOr(errw, PRED_ERR_PRECISION);
+                    }
+                }
+                out[i] = (int8_t)f;
+            }
+        }
+    }
+}
+
+void launch_eval_pred(const Launch& L, int kind, const double* pts, const int* idx, int count, int8_t* out,
+                      unsigned* err) {
+    int b = (count + 127) / 128;
+    if (b > 148 * 8) b = 148 * 8;
+    k_eval_pred<<<b < 1 ? 1 : b, 128, 0, L.stream>>>(kind, pts, idx, count, out, err);
+    ++*L.launches;
+}
+
+// --------------------------------------------------------------------------
+
+static int star_blocks(int items) {
+    int b = (items + WARPS_PER_BLOCK - 1) / WARPS_PER_BLOCK;
+    const int cap = 148 * 8;
+    if (b > cap) b = cap;
+    return b < 1 ? 1 : b;
+}
+
+static size_t ws_bytes() { return sizeof(WS) * WARPS_PER_BLOCK; }
+
+void launch_star_build(const Launch& L, const Dev& D) {
+    cudaFuncSetAttribute(k_star_build, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ws_bytes());
+    k_star_build<<<star_blocks(D.n), 32 * WARPS_PER_BLOCK, ws_bytes(), L.stream>>>(D);
+    ++*L.launches;
+}
+
+void launch_star_insert(const Launch& L, const Dev& D, int count) {
+    cudaFuncSetAttribute(k_star_insert, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ws_bytes());
+    k_star_insert<<<star_blocks(count), 32 * WARPS_PER_BLOCK, ws_bytes(), L.stream>>>(D, count);
+    ++*L.launches;
+}
+
+void launch_emit(const Launch& L, const Dev& D, int count) {
+    k_emit<<<star_blocks(count), 32 * WARPS_PER_BLOCK, 0, L.stream>>>(D, count);
+    ++*L.launches;
+}
+
+void launch_proof(const Launch& L, const Dev& D, int count) {
+    k_proof<<<star_blocks(count), 32 * WARPS_PER_BLOCK, 0, L.stream>>>(D, count);
+    ++*L.launches;
+}
+
+void launch_check(const Launch& L, const Dev& D, unsigned long long* bad) {
+    k_check<<<star_blocks(D.n), 32 * WARPS_PER_BLOCK, 0, L.stream>>>(D, bad);
+    ++*L.launches;
+}
+
+void launch_tet_count(const Launch& L, const Dev& D, int* cnt) {
+    k_tet_count<<<star_blocks(D.n), 32 * WARPS_PER_BLOCK, 0, L.stream>>>(D, cnt);
+    ++*L.launches;
+}
+
+void launch_tet_write(const Launch& L, const Dev& D, const int* base, g4d_tet* tets, const int* sorted_to_input) {
+    k_tet_write<<<star_blocks(D.n), 32 * WARPS_PER_BLOCK, 0, L.stream>>>(D, base, tets, sorted_to_input);
+    ++*L.launches;
+}
+#endif  // G4D_HOST_EMULATION
+
+}  // namespace g4d

@@ -1,0 +1,156 @@
+/*
+ * gStar4D-B200: C ABI of the B200-native 3D Delaunay triangulator.
+ *
+ * Point cloud in (FP64 x,y,z), tetrahedra with adjacency out. The entry points
+ * below replace the reference's C++ facade (GDelaunay/GDelaunay.h:39-42,
+ * GDelaunay/GDelaunay.cpp:47-104) with plain C types: status codes instead of
+ * exit(-1), caller buffers never mutated unless the reference mutates them too,
+ * one context per host thread instead of process-wide globals.
+ *
+ * Semantics shared with the reference:
+ *  - Point indices in the output are either input indices (default) or the
+ *    Morton-sorted order the reference reports (GDelData.cu:91-134).
+ *  - Tetrahedron layout equals the reference's Tetrahedron (Common/Geometry.h:
+ *    147-150): v[0..2] = owner link triangle, v[3] = owner star (the smallest
+ *    vertex), orient3d(v0,v1,v2,v3) < 0 (GDelPredKernels.cu:628-665), opp[i] =
+ *    index of the tetrahedron across the face opposite v[i], -1 if there is none.
+ *  - The tetrahedra are the Delaunay tetrahedra under the reference's
+ *    Simulation of Simplicity by Morton index (GDelPredDevice.h:142-698);
+ *    zero-volume tetrahedra are dropped as in the reference.
+ */
+#ifndef GSTAR4D_H
+#define GSTAR4D_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define G4D_API __attribute__((visibility("default")))
+#else
+#define G4D_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    G4D_OK = 0,
+    G4D_ERR_ARG = 1,        /* invalid argument (sizes, grid, NULL pointers, duplicate points) */
+    G4D_ERR_NOMEM = 2,      /* device or host allocation failed */
+    G4D_ERR_TIMEOUT = 3,    /* an iteration cap was reached (splaying did not converge) */
+    G4D_ERR_INTERNAL = 4,   /* an internal consistency check failed */
+    G4D_ERR_CUDA = 5,       /* a CUDA runtime call failed */
+    G4D_ERR_CAPACITY = 6,   /* a star outgrew the largest supported star size */
+    G4D_ERR_PRECISION = 7,  /* coordinates span too wide a binary exponent range */
+    G4D_ERR_NODEVICE = 8    /* no CUDA device, or the device is not sm_100 */
+} g4d_status;
+
+/* Mirrors the reference's Config (Common/Config.h:59-79) plus the B200 options. */
+typedef struct {
+    int seed;            /* -s   (CLI point generation) */
+    int run_num;         /* -r */
+    int grid_size;       /* -g   PBA grid width G: power of two, 32..1024; 0 = autotune */
+    int point_num;       /* -n */
+    int dist;            /* -d   0 uniform, 1 gaussian, 2 ball, 3 sphere, 4 grid */
+    int facet_max;       /* -f   kept for flag compatibility (no effect: no per-loop bound) */
+    int log_verbose;     /* -verbose */
+    int log_stats;       /* -stats */
+    int log_timing;      /* -timing */
+    int do_check;        /* -check: device star-consistency check after splaying */
+    int pred_thread_num; /* -predThreadNum (kept for flag compatibility) */
+    int pred_block_num;  /* -predBlockNum  (kept for flag compatibility) */
+    int do_sorting;      /* -sort (always on: Morton order defines the SoS ranks) */
+    int device;          /* CUDA device ordinal */
+    int index_space;     /* 0: output indices are input indices; 1: Morton-sorted indices */
+    int proposal;        /* 0: plain PBA stars; 1: learned star proposal (needs a model) */
+} g4d_config;
+
+/* == Tetrahedron of Common/Geometry.h:147-150 */
+typedef struct {
+    int v[4];
+    int opp[4];
+} g4d_tet;
+
+typedef struct {
+    double t_init_ms, t_pba_ms, t_star_ms, t_splay_ms, t_out_ms, t_total_ms;
+    long long star_insertions;   /* initial worksets inserted (LogStarInsNum) */
+    long long splay_insertions;  /* insertions during splaying (LogSplayInsNum) */
+    long long drowned, proofs, exact_predicates;
+    int loops;                   /* splaying loops (LogLoopNum) */
+    int missing;                 /* points absent from the digital Voronoi diagram */
+    int grid_size;               /* grid actually used */
+    int tets;
+    long long gpu_launches;      /* kernels launched by this call */
+} g4d_stats;
+
+typedef struct g4d_ctx g4d_ctx;
+
+/* Defaults: grid 0 (autotune), index_space 0, device 0, sorting on. */
+G4D_API void g4d_default_config(g4d_config* cfg);
+
+/* Replaces the reference's process-wide state set up by gdelInit/starsInit
+ * (GDelHost.cu:136-234): one context owns a device, a stream and workspace. */
+G4D_API g4d_status g4d_create(g4d_ctx** ctx, const g4d_config* cfg);
+G4D_API void g4d_destroy(g4d_ctx* ctx);
+G4D_API const char* g4d_last_error(const g4d_ctx* ctx);
+G4D_API const char* g4d_status_string(g4d_status s);
+
+/* One triangulation from host memory (gdelInit + gdelCompute + getTetraFromGpu,
+ * GDelaunay.cpp:47-96, with Application::_scalePoint scaling, Application.cpp:
+ * 589-603, of the FP64 points into grid units). xyz: n*3 doubles, input order,
+ * not modified. *tets is allocated by the library (free with g4d_free).
+ * sorted_to_input (optional, n ints): Morton position -> input index. */
+G4D_API g4d_status g4d_triangulate(g4d_ctx* ctx, const double* xyz, int n, g4d_tet** tets, int* ntet,
+                           int* sorted_to_input, g4d_stats* stats);
+
+/* Same as g4d_triangulate but into a caller buffer (e.g. pinned host memory):
+ * out may be NULL to query *ntet; returns G4D_ERR_ARG with *ntet set when cap
+ * is too small. */
+G4D_API g4d_status g4d_triangulate_to(g4d_ctx* ctx, const double* xyz, int n, g4d_tet* out, int cap, int* ntet,
+                              int* sorted_to_input, g4d_stats* stats);
+
+/* Same on device memory (inputs already resident in HBM, output left there).
+ * d_xyz: n*3 doubles on ctx's device. The tetrahedra stay in a context-owned
+ * device buffer returned through *d_tets (valid until the next call). */
+G4D_API g4d_status g4d_triangulate_device(g4d_ctx* ctx, const double* d_xyz, int n, const g4d_tet** d_tets,
+                                  int* ntet, g4d_stats* stats);
+
+/* Reference-shaped entry points (GDelaunay.h:39-42).
+ * g4d_gdel_init: points (n*3) are the predicate coordinates; scaled (n*3 grid
+ * units in [1, G-2], or NULL when points are already in grid units) feeds the
+ * grid and the Morton order. Like gdelInit (GDelData.cu:125-130) both arrays
+ * are overwritten with the Morton-sorted order. */
+G4D_API g4d_status g4d_gdel_init(g4d_ctx* ctx, double* points, double* scaled, int n);
+/* gdelCompute: stage times in milliseconds (PBA, initial stars, splaying, output). */
+G4D_API g4d_status g4d_gdel_compute(g4d_ctx* ctx, double* t_pba, double* t_star, double* t_splay, double* t_out);
+/* getTetraFromGpu: tetrahedra in Morton-sorted indices; pointer valid until the
+ * next compute or deinit. */
+G4D_API g4d_status g4d_get_tetra(g4d_ctx* ctx, const g4d_tet** tets, int* ntet);
+G4D_API g4d_status g4d_gdel_deinit(g4d_ctx* ctx);
+
+/* Batched triangulation of many clouds in one pass (persistent kernels over a
+ * per-cloud work queue). xyz holds all clouds back to back; cloud c spans
+ * points [cloud_offsets[c], cloud_offsets[c+1]). Tetrahedra of cloud c are
+ * tets[tet_offsets[c] .. tet_offsets[c+1]) with cloud-local point indices.
+ * *tets and *tet_offsets are library-allocated (g4d_free). */
+G4D_API g4d_status g4d_triangulate_batch(g4d_ctx* ctx, const double* xyz, const int64_t* cloud_offsets, int nclouds,
+                                 g4d_tet** tets, int64_t** tet_offsets, g4d_stats* stats);
+
+/* Diagnostic: evaluates the device predicates on `count` point sets (host
+ * arrays). kind 0: orient3d sign of 4 points (12 doubles per set);
+ * kind 1: lifted orient4 sign with Simulation of Simplicity (15 doubles and 5
+ * indices per set); kind 2: orient4 without SoS (0 when degenerate). */
+G4D_API g4d_status g4d_eval_predicates(g4d_ctx* ctx, int kind, const double* pts, const int* idx, int count,
+                                       int8_t* out);
+
+/* The context's CUDA stream (a cudaStream_t), for callers that time or order
+ * their own work against the library's launches. */
+G4D_API void* g4d_stream(g4d_ctx* ctx);
+
+G4D_API void g4d_free(void* p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

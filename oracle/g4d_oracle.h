@@ -36,6 +36,7 @@ typedef struct {
     long long voronoi_pairs, workset_total, star_insertions, splay_insertions;
     long long drowned, proofs, exact_calls, consistency_repairs;
     double t_order, t_pba, t_star, t_splay, t_out, t_total;
+    int max_hist;
 } ora_stats;
 
 /* Status codes (same meaning as the product's G4D_* codes). */

@@ -31,6 +31,7 @@ class OraStats(ctypes.Structure):
         ("exact_calls", ctypes.c_longlong), ("consistency_repairs", ctypes.c_longlong),
         ("t_order", ctypes.c_double), ("t_pba", ctypes.c_double), ("t_star", ctypes.c_double),
         ("t_splay", ctypes.c_double), ("t_out", ctypes.c_double), ("t_total", ctypes.c_double),
+        ("max_hist", ctypes.c_int),
     ]
 
     def as_dict(self):

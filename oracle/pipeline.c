@@ -771,6 +771,8 @@ int ora_triangulate(const double* xyz, int n, int G, int nthreads, int input_ord
         if (S->nt > maxl) maxl = S->nt;
     }
     st->max_link = (maxl + 4) / 2;
+    for (int s = 0; s < n; ++s)
+        if (C.S[s].hist.n > st->max_hist) st->max_hist = C.S[s].hist.n;
     const int nown = base[n];
     ora_tet* tets = (ora_tet*)malloc(sizeof(ora_tet) * (nown ? nown : 1));
     unsigned char* keep = (unsigned char*)calloc(nown ? nown : 1, 1);
