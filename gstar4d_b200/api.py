@@ -59,7 +59,7 @@ _lib = None
 EXPORTS = ["g4d_default_config", "g4d_create", "g4d_destroy", "g4d_last_error", "g4d_status_string",
            "g4d_triangulate", "g4d_triangulate_to", "g4d_triangulate_device", "g4d_gdel_init",
            "g4d_gdel_compute", "g4d_get_tetra", "g4d_gdel_deinit", "g4d_triangulate_batch", "g4d_stream",
-           "g4d_eval_predicates", "g4d_free"]
+           "g4d_eval_predicates", "g4d_voronoi", "g4d_free"]
 
 
 def load():
@@ -88,6 +88,7 @@ def load():
     L.g4d_triangulate_batch.argtypes = [vp, vp, vp, ip, ctypes.POINTER(vp), ctypes.POINTER(vp),
                                         ctypes.POINTER(Stats)]
     L.g4d_eval_predicates.argtypes = [vp, ip, vp, vp, ip, vp]
+    L.g4d_voronoi.argtypes = [vp, vp, ip, ip, vp]
     L.g4d_stream.argtypes = [vp]
     L.g4d_stream.restype = vp
     L.g4d_free.argtypes = [vp]
@@ -193,6 +194,13 @@ class Triangulator:
         st = self._lib.g4d_eval_predicates(self._h, int(kind), _ptr(pts), _ptr(ia) if ia is not None else None,
                                            count, _ptr(out))
         self._check(st)
+        return out
+
+    def voronoi(self, points, grid):
+        """Digital Voronoi grid (grid^3 packed site voxels, x fastest)."""
+        pts = np.ascontiguousarray(points, dtype=np.float64)
+        out = np.empty(grid ** 3, np.uint32)
+        self._check(self._lib.g4d_voronoi(self._h, _ptr(pts), len(pts), int(grid), _ptr(out)))
         return out
 
     # ---- reference-shaped entry points ------------------------------------------------

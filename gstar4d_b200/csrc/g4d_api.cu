@@ -633,6 +633,31 @@ g4d_status g4d_eval_predicates(g4d_ctx* ctx, int kind, const double* pts, const 
     return G4D_OK;
 }
 
+g4d_status g4d_voronoi(g4d_ctx* ctx, const double* xyz, int n, int grid, uint32_t* sites) {
+    g4d_status st = check_n(ctx, n);
+    if (st) return st;
+    if (!xyz || !sites) return fail(ctx, G4D_ERR_ARG, "null argument");
+    if (grid < 32 || grid > 1024 || (grid & (grid - 1))) return fail(ctx, G4D_ERR_ARG, "bad grid %d", grid);
+    cudaSetDevice(ctx->device);
+    ctx->n = n;
+    ctx->G = grid;
+    const size_t G3 = (size_t)grid * grid * grid;
+    CK(ctx->b[B_XYZ].ensure(sizeof(double) * 3 * (size_t)n));
+    CK(cudaMemcpyAsync(ctx->b[B_XYZ].p, xyz, sizeof(double) * 3 * (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
+    st = run_order(ctx, ctx->b[B_XYZ].as<double>(), nullptr, n);
+    if (st) return st;
+    CK(ctx->b[B_GA].ensure(sizeof(uint32_t) * G3));
+    CK(ctx->b[B_GB].ensure(sizeof(uint32_t) * G3));
+    Launch L{ctx->stream, &ctx->launches};
+    Dev D = make_dev(ctx);
+    launch_pba_z(L, D, ctx->b[B_GA].as<uint32_t>());
+    launch_pba_y(L, grid, ctx->b[B_GA].as<uint32_t>(), ctx->b[B_GB].as<uint32_t>());
+    launch_pba_x(L, grid, ctx->b[B_GB].as<uint32_t>(), ctx->b[B_GA].as<uint32_t>());
+    CK(cudaMemcpyAsync(sites, ctx->b[B_GA].p, sizeof(uint32_t) * G3, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return G4D_OK;
+}
+
 void* g4d_stream(g4d_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 
 void g4d_free(void* p) { free(p); }

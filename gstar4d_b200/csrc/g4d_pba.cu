@@ -45,21 +45,28 @@ __global__ void __launch_bounds__(128) k_pba_z(int G, const uint32_t* __restrict
     }
 }
 
-// y pass: tile[y][tx], TX consecutive x at fixed z
+// y pass: TX consecutive x-columns at fixed z. The slab is staged transposed
+// (one line per x, pitch G+1 so the transposing stores are conflict-free), a
+// warp resolves 32 consecutive voxels of one line (neighbouring voxels have
+// similar search lengths, so the warp stays converged), and results go
+// through a second, row-major tile so the global stores are coalesced.
 template <int TX>
 __global__ void __launch_bounds__(256) k_pba_y(int G, const uint32_t* __restrict__ in, uint32_t* __restrict__ out) {
-    extern __shared__ uint32_t tile[];
+    extern __shared__ uint32_t smem_pba[];
+    uint32_t* lines = smem_pba;                     // [TX][G+1]
+    uint32_t* res = smem_pba + (size_t)TX * (G + 1);  // [G][TX+1]
     const int x0 = blockIdx.x * TX;
     const int z = blockIdx.y;
     const size_t zoff = (size_t)z * G * G;
     const int total = G * TX;
     for (int k = threadIdx.x; k < total; k += blockDim.x) {
         const int yy = k / TX, xx = k % TX;
-        tile[k] = in[zoff + (size_t)yy * G + x0 + xx];
+        lines[xx * (G + 1) + yy] = in[zoff + (size_t)yy * G + x0 + xx];
     }
     __syncthreads();
     for (int k = threadIdx.x; k < total; k += blockDim.x) {
-        const int y = k / TX, xx = k % TX;
+        const int xx = k / G, y = k % G;
+        const uint32_t* line = lines + xx * (G + 1);
         uint32_t best = MARKER;
         int bestd = 0x7fffffff;
         for (int d = 0;; ++d) {
@@ -67,7 +74,7 @@ __global__ void __launch_bounds__(256) k_pba_y(int G, const uint32_t* __restrict
             const int ya = y - d, yb = y + d;
             if (ya < 0 && yb >= G) break;
             if (ya >= 0) {
-                const uint32_t s = tile[ya * TX + xx];
+                const uint32_t s = line[ya];
                 if (s != MARKER) {
                     const int dz = z - (int)vz(s);
                     const int dd = d * d + dz * dz;
@@ -75,7 +82,7 @@ __global__ void __launch_bounds__(256) k_pba_y(int G, const uint32_t* __restrict
                 }
             }
             if (d > 0 && yb < G) {
-                const uint32_t s = tile[yb * TX + xx];
+                const uint32_t s = line[yb];
                 if (s != MARKER) {
                     const int dz = z - (int)vz(s);
                     const int dd = d * d + dz * dz;
@@ -83,7 +90,12 @@ __global__ void __launch_bounds__(256) k_pba_y(int G, const uint32_t* __restrict
                 }
             }
         }
-        out[zoff + (size_t)y * G + x0 + xx] = best;
+        res[y * (TX + 1) + xx] = best;
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < total; k += blockDim.x) {
+        const int yy = k / TX, xx = k % TX;
+        out[zoff + (size_t)yy * G + x0 + xx] = res[yy * (TX + 1) + xx];
     }
 }
 
@@ -144,55 +156,86 @@ __device__ __forceinline__ void push_bucket(const Dev& D, int a, int b) {
     if (pos < BUCKET_CAP) D.bucket[(size_t)a * BUCKET_CAP + pos] = b;
 }
 
-constexpr int PAIR_HASH = 2048;
-constexpr int PAIR_ZC = 8;
+constexpr int PAIR_HASH = 4096;
+constexpr int PAIR_PROBES = 32;
+constexpr int PAIR_ZC = 16;
 
-// Every two distinct sites meeting in a 2x2x2 voxel cube are a candidate
-// Delaunay edge (the reference reads the same cubes, GDelKernels.cu:137-299).
-// Block-local dedupe in a shared-memory hash before the per-star scatter.
-__global__ void __launch_bounds__(256) k_pairs(Dev D, const uint32_t* __restrict__ grid) {
+__device__ __forceinline__ void pair_hash_insert(unsigned long long* hs, unsigned long long key, const Dev& D) {
+    unsigned h = (unsigned)((key * 0x9E3779B97F4A7C15ull) >> 52) & (PAIR_HASH - 1);
+    for (int probe = 0; probe < PAIR_PROBES; ++probe) {
+        const unsigned long long old = atomicCAS(&hs[h], ~0ull, key);
+        if (old == ~0ull || old == key) return;
+        h = (h + 1) & (PAIR_HASH - 1);
+    }
+    // crowded table (dense regions hold thousands of pairs per block): emit
+    // directly instead of probing further
+    const int ia = site_to_id(D, (uint32_t)(key >> 32)), ib = site_to_id(D, (uint32_t)key);
+    if (ia >= 0 && ib >= 0) { push_bucket(D, ia, ib); push_bucket(D, ib, ia); }
+}
+
+// Candidate Delaunay edges: every two distinct sites of a 2x2x2 voxel cube in
+// which at least three sites meet (a digital Voronoi edge or vertex; the
+// reference reads the same cubes and emits around digital Voronoi vertices,
+// GDelKernels.cu:137-299). One thread sweeps a column of cubes along z,
+// keeping the previous voxel plane in registers (4 new loads per cube,
+// coalesced over x); a per-thread cache of the last pairs and a block-local
+// hash remove duplicates before the per-star scatter.
+__global__ void __launch_bounds__(128) k_pairs(Dev D, const uint32_t* __restrict__ grid) {
     __shared__ unsigned long long hs[PAIR_HASH];
     const int G = D.G;
-    for (int k = threadIdx.y * 32 + threadIdx.x; k < PAIR_HASH; k += 256) hs[k] = ~0ull;
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    for (int k = tid; k < PAIR_HASH; k += 128) hs[k] = ~0ull;
     __syncthreads();
     const int x = blockIdx.x * 32 + threadIdx.x;
-    const int y = blockIdx.y * 8 + threadIdx.y;
+    const int y = blockIdx.y * 4 + threadIdx.y;
     const int z0 = blockIdx.z * PAIR_ZC;
     const size_t plane = (size_t)G * G;
-    if (x < G - 1 && y < G - 1) {
-        for (int zi = 0; zi < PAIR_ZC; ++zi) {
-            const int z = z0 + zi;
-            if (z >= G - 1) break;
+    const int lane = threadIdx.x;
+    // every lane of the warp walks the same z range so the warp collectives
+    // below stay converged; lanes past the grid edge carry no pairs
+    const bool active = x < G - 1 && y < G - 1;
+    const int zend = min(z0 + PAIR_ZC, G - 1);
+    if (y < G - 1 && z0 < G - 1) {
+        const uint32_t* g = grid + (size_t)y * G + (active ? x : 0);
+        uint32_t a0 = g[(size_t)z0 * plane], a1 = g[(size_t)z0 * plane + 1];
+        uint32_t a2 = g[(size_t)z0 * plane + G], a3 = g[(size_t)z0 * plane + G + 1];
+        unsigned long long recent[4] = {~0ull, ~0ull, ~0ull, ~0ull};
+        int rp = 0;
+        for (int z = z0; z < zend; ++z) {
+            const size_t o = (size_t)(z + 1) * plane;
+            const uint32_t b0 = g[o], b1 = g[o + 1], b2 = g[o + G], b3 = g[o + G + 1];
+            const uint32_t v[8] = {a0, a1, a2, a3, b0, b1, b2, b3};
             uint32_t s[8];
             int ns = 0;
-            for (int dz = 0; dz < 2; ++dz)
-                for (int dy = 0; dy < 2; ++dy)
-                    for (int dx = 0; dx < 2; ++dx) {
-                        const uint32_t v = __ldg(&grid[(size_t)(z + dz) * plane + (size_t)(y + dy) * G + x + dx]);
-                        bool dup = false;
-                        for (int k = 0; k < ns; ++k) dup |= (s[k] == v);
-                        if (!dup) s[ns++] = v;
-                    }
-            for (int a = 0; a < ns; ++a)
-                for (int b = a + 1; b < ns; ++b) {
-                    const uint32_t lo = s[a] < s[b] ? s[a] : s[b], hi = s[a] < s[b] ? s[b] : s[a];
-                    const unsigned long long key = ((unsigned long long)lo << 32) | hi;
-                    unsigned h = (unsigned)((key * 0x9E3779B97F4A7C15ull) >> 53) & (PAIR_HASH - 1);
-                    bool placed = false;
-                    for (int probe = 0; probe < PAIR_HASH; ++probe) {
-                        const unsigned long long old = atomicCAS(&hs[h], ~0ull, key);
-                        if (old == ~0ull || old == key) { placed = true; break; }
-                        h = (h + 1) & (PAIR_HASH - 1);
-                    }
-                    if (!placed) {  // table full: emit directly
-                        const int ia = site_to_id(D, lo), ib = site_to_id(D, hi);
-                        if (ia >= 0 && ib >= 0) { push_bucket(D, ia, ib); push_bucket(D, ib, ia); }
-                    }
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                bool dup = false;
+                for (int k = 0; k < ns; ++k) dup |= (s[k] == v[i]);
+                if (!dup) s[ns++] = v[i];
+            }
+            const int np = (active && ns >= 3) ? ns * (ns - 1) / 2 : 0;
+            const int maxp = __reduce_max_sync(0xffffffffu, (unsigned)np);
+            int pi = 0, pj = 1;
+            for (int k = 0; k < maxp; ++k) {
+                unsigned long long key = ~0ull;
+                if (k < np) {
+                    const uint32_t lo = s[pi] < s[pj] ? s[pi] : s[pj], hi = s[pi] < s[pj] ? s[pj] : s[pi];
+                    key = ((unsigned long long)lo << 32) | hi;
+                    if (++pj == ns) { ++pi; pj = pi + 1; }
+                    if (key == recent[0] || key == recent[1] || key == recent[2] || key == recent[3])
+                        key = ~0ull;
+                    else
+                        recent[(rp++) & 3] = key;
                 }
+                // lanes holding the same pair elect one inserter
+                const unsigned grp = __match_any_sync(0xffffffffu, key);
+                if (key != ~0ull && lane == __ffs(grp) - 1) pair_hash_insert(hs, key, D);
+            }
+            a0 = b0; a1 = b1; a2 = b2; a3 = b3;
         }
     }
     __syncthreads();
-    for (int k = threadIdx.y * 32 + threadIdx.x; k < PAIR_HASH; k += 256) {
+    for (int k = tid; k < PAIR_HASH; k += 128) {
         const unsigned long long key = hs[k];
         if (key == ~0ull) continue;
         const int ia = site_to_id(D, (uint32_t)(key >> 32)), ib = site_to_id(D, (uint32_t)key);
@@ -223,16 +266,18 @@ void launch_pba_z(const Launch& L, const Dev& D, uint32_t* out) {
 }
 
 void launch_pba_y(const Launch& L, int G, const uint32_t* in, uint32_t* out) {
-    if (G >= 1024) {
-        constexpr int TX = 16;
-        const size_t sm = (size_t)G * TX * 4;
-        cudaFuncSetAttribute(k_pba_y<TX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        k_pba_y<TX><<<dim3(G / TX, G), 256, sm, L.stream>>>(G, in, out);
-    } else {
-        constexpr int TX = 32;
-        const size_t sm = (size_t)G * TX * 4;
-        cudaFuncSetAttribute(k_pba_y<TX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        k_pba_y<TX><<<dim3(G / TX, G), 256, sm, L.stream>>>(G, in, out);
+    // two tiles of TX*G voxels: 64 KB for G >= 256
+    const int TX = G >= 1024 ? 8 : (G >= 512 ? 16 : 32);
+    const size_t sm = ((size_t)TX * (G + 1) + (size_t)G * (TX + 1)) * 4;
+    switch (TX) {
+#define G4D_Y(T)                                                                                  \
+    case T:                                                                                       \
+        cudaFuncSetAttribute(k_pba_y<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm); \
+        k_pba_y<T><<<dim3(G / T, G), 256, sm, L.stream>>>(G, in, out);                            \
+        break;
+        G4D_Y(8) G4D_Y(16) G4D_Y(32)
+#undef G4D_Y
+        default: break;
     }
     ++*L.launches;
 }
@@ -256,7 +301,7 @@ void launch_pba_x(const Launch& L, int G, const uint32_t* in, uint32_t* out) {
 
 void launch_pairs(const Launch& L, const Dev& D, const uint32_t* grid) {
     const int G = D.G;
-    dim3 b(32, 8), g((G - 1 + 31) / 32, (G - 1 + 7) / 8, (G - 1 + PAIR_ZC - 1) / PAIR_ZC);
+    dim3 b(32, 4), g((G - 1 + 31) / 32, (G - 1 + 3) / 4, (G - 1 + PAIR_ZC - 1) / PAIR_ZC);
     k_pairs<<<g, b, 0, L.stream>>>(D, grid);
     ++*L.launches;
 }

@@ -441,7 +441,9 @@ __device__ void warp_store(WS& S, const Dev& D, int lane, int s, int pass, bool 
 // build: initial star of every point from its candidate workset
 // --------------------------------------------------------------------------
 
-__global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_star_build(Dev D) {
+// 3 blocks per SM: shared memory (about 65 KB per block) allows no more, and
+// this register budget (168) costs only a few hundred bytes of spills.
+__global__ void __launch_bounds__(32 * WARPS_PER_BLOCK, 3) k_star_build(Dev D) {
     G4D_DYN_SMEM(smem_raw);
     const int lane = threadIdx.x & 31;
     WS& S = reinterpret_cast<WS*>(smem_raw)[threadIdx.x >> 5];
@@ -541,7 +543,7 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_star_build(Dev D) {
 // insertion round: every star with inbox requests
 // --------------------------------------------------------------------------
 
-__global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_star_insert(Dev D, int count) {
+__global__ void __launch_bounds__(32 * WARPS_PER_BLOCK, 3) k_star_insert(Dev D, int count) {
     G4D_DYN_SMEM(smem_raw);
     const int lane = threadIdx.x & 31;
     WS& S = reinterpret_cast<WS*>(smem_raw)[threadIdx.x >> 5];

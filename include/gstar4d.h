@@ -144,6 +144,12 @@ G4D_API g4d_status g4d_triangulate_batch(g4d_ctx* ctx, const double* xyz, const 
 G4D_API g4d_status g4d_eval_predicates(g4d_ctx* ctx, int kind, const double* pts, const int* idx, int count,
                                        int8_t* out);
 
+/* Diagnostic: the digital Voronoi diagram the star construction starts from
+ * (PBA output, PBA/Pba.cu:105-122 doPba). xyz as in g4d_triangulate; sites
+ * receives grid^3 values, voxel (x,y,z) at ((z*grid)+y)*grid+x, each the packed
+ * voxel x | y<<10 | z<<20 of its nearest site (0xffffffff if none). */
+G4D_API g4d_status g4d_voronoi(g4d_ctx* ctx, const double* xyz, int n, int grid, uint32_t* sites);
+
 /* The context's CUDA stream (a cudaStream_t), for callers that time or order
  * their own work against the library's launches. */
 G4D_API void* g4d_stream(g4d_ctx* ctx);

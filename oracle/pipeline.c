@@ -359,8 +359,10 @@ static int find_proof(const double* P, const ostar* s, int star, int inv, int* p
 /* Pairs from the digital Voronoi diagram                                    */
 /* ------------------------------------------------------------------------- */
 
-/* Candidate Delaunay edges: every two distinct sites that meet in a 2x2x2 voxel
- * cube (the reference reads the same cubes, GDelKernels.cu:137-299). */
+/* Candidate Delaunay edges: every two distinct sites of a 2x2x2 voxel cube in
+ * which at least three sites meet (a digital Voronoi edge or vertex). The
+ * reference reads the same cubes and emits around digital Voronoi vertices
+ * (GDelKernels.cu:137-299). */
 static void grid_pairs(const int* site, int G, lvec* out) {
     const int nt = omp_get_max_threads();
     lvec* per = (lvec*)calloc(nt, sizeof(lvec));
@@ -384,6 +386,7 @@ static void grid_pairs(const int* site, int G, lvec* out) {
                             for (int k = 0; k < ns; ++k) if (s[k] == v) { dup = 1; break; }
                             if (!dup) s[ns++] = v;
                         }
+                if (ns < 3) continue; /* only digital Voronoi edges and vertices */
                 for (int a = 0; a < ns; ++a)
                     for (int b = a + 1; b < ns; ++b) {
                         const int lo = s[a] < s[b] ? s[a] : s[b], hi = s[a] < s[b] ? s[b] : s[a];

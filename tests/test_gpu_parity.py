@@ -92,6 +92,26 @@ def test_morton_index_space_and_gdel_entry_points(oracle):
     assert np.array_equal(g[0], r[0])
 
 
+@pytest.mark.parametrize("kind,n,G", [("mixed", 20000, 64), ("uniform", 100000, 256), ("clustered", 50000, 128)])
+def test_voronoi_grid_is_exact(tri, oracle, kind, n, G):
+    """Every voxel's PBA site is at the exact minimum squared distance."""
+    pts = {"mixed": workloads.mixed, "uniform": workloads.uniform, "clustered": workloads.clustered}[kind](n, seed=6)
+    sites = tri.voronoi(pts, G)
+    _, vox = oracle.morton_order(pts, G)
+    ref = oracle.edt(vox, G)
+    g = np.arange(G)
+    Z, Y, X = np.meshgrid(g, g, g, indexing="ij")
+    sx, sy, sz = (sites & 1023).astype(np.int64), ((sites >> 10) & 1023).astype(np.int64), ((sites >> 20) & 1023).astype(np.int64)
+    d_gpu = (sx - X.ravel()) ** 2 + (sy - Y.ravel()) ** 2 + (sz - Z.ravel()) ** 2
+    rv = vox[ref].astype(np.int64)
+    d_ref = (rv[:, 0] - X.ravel()) ** 2 + (rv[:, 1] - Y.ravel()) ** 2 + (rv[:, 2] - Z.ravel()) ** 2
+    assert (sites != 0xFFFFFFFF).all()
+    assert np.array_equal(d_gpu, d_ref)
+    # every site is an occupied voxel
+    occ = set((vox[:, 0] | (vox[:, 1] << 10) | (vox[:, 2] << 20)).tolist())
+    assert set(np.unique(sites).tolist()) <= occ
+
+
 def test_invalid_arguments_raise(tri):
     import gstar4d_b200
     with pytest.raises(gstar4d_b200.G4DError) as e:
