@@ -59,7 +59,7 @@ _lib = None
 EXPORTS = ["g4d_default_config", "g4d_create", "g4d_destroy", "g4d_last_error", "g4d_status_string",
            "g4d_triangulate", "g4d_triangulate_to", "g4d_triangulate_device", "g4d_gdel_init",
            "g4d_gdel_compute", "g4d_get_tetra", "g4d_gdel_deinit", "g4d_triangulate_batch", "g4d_stream",
-           "g4d_eval_predicates", "g4d_voronoi", "g4d_free"]
+           "g4d_eval_predicates", "g4d_voronoi", "g4d_voronoi_noalloc", "g4d_free"]
 
 
 def load():
@@ -89,6 +89,7 @@ def load():
                                         ctypes.POINTER(Stats)]
     L.g4d_eval_predicates.argtypes = [vp, ip, vp, vp, ip, vp]
     L.g4d_voronoi.argtypes = [vp, vp, ip, ip, vp]
+    L.g4d_voronoi_noalloc.argtypes = [vp, ip, ip, vp, vp]
     L.g4d_stream.argtypes = [vp]
     L.g4d_stream.restype = vp
     L.g4d_free.argtypes = [vp]

@@ -150,6 +150,21 @@ G4D_API g4d_status g4d_eval_predicates(g4d_ctx* ctx, int kind, const double* pts
  * voxel x | y<<10 | z<<20 of its nearest site (0xffffffff if none). */
 G4D_API g4d_status g4d_voronoi(g4d_ctx* ctx, const double* xyz, int n, int grid, uint32_t* sites);
 
+/* No counterpart in the reference. g4d_voronoi without any device allocation,
+ * for callers that cannot allocate GPU memory (device memory owned by a host
+ * framework's pool, or loops where cudaMalloc/cudaFree and their implicit
+ * synchronization are not allowed). d_xyz (n*3 doubles) and d_sites (grid^3
+ * values, layout as g4d_voronoi) are DEVICE pointers owned by the caller;
+ * stream is a cudaStream_t (NULL: the legacy default stream). The work is
+ * enqueued on that stream and the call returns without synchronizing.
+ * Scratch is one fixed device array in the library (about 11.5 MB per device),
+ * so n is at most 262144 and grid at most 128; larger sizes return
+ * G4D_ERR_CAPACITY (with a message on stderr) and enqueue nothing. Every call
+ * shares that array: calls that overlap on the GPU (other streams or threads)
+ * race and must be serialized by the caller. The first call on each device
+ * looks up the array's address; make it outside any stream capture. */
+G4D_API g4d_status g4d_voronoi_noalloc(const double* d_xyz, int n, int grid, uint32_t* d_sites, void* stream);
+
 /* The context's CUDA stream (a cudaStream_t), for callers that time or order
  * their own work against the library's launches. */
 G4D_API void* g4d_stream(g4d_ctx* ctx);
