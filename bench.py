@@ -263,7 +263,8 @@ def main():
             "stages_ms": {k: round(last[k], 3) for k in ("t_init_ms", "t_pba_ms", "t_star_ms", "t_splay_ms",
                                                           "t_out_ms", "t_total_ms")},
             "splay": {"loops": last["loops"], "insertions": last["splay_insertions"], "proofs": last["proofs"],
-                      "exact_predicates": last["exact_predicates"], "tets": ntets},
+                      "exact_predicates": last["exact_predicates"], "large_stars": last["large_stars"],
+                      "tets": ntets},
             "clocks": clocks,
             "gpu_launches": int(launches),
         }

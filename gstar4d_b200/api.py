@@ -46,7 +46,8 @@ class Stats(ctypes.Structure):
                 ("star_insertions", ctypes.c_longlong), ("splay_insertions", ctypes.c_longlong),
                 ("drowned", ctypes.c_longlong), ("proofs", ctypes.c_longlong),
                 ("exact_predicates", ctypes.c_longlong), ("loops", ctypes.c_int), ("missing", ctypes.c_int),
-                ("grid_size", ctypes.c_int), ("tets", ctypes.c_int), ("gpu_launches", ctypes.c_longlong)]
+                ("grid_size", ctypes.c_int), ("tets", ctypes.c_int), ("gpu_launches", ctypes.c_longlong),
+                ("large_stars", ctypes.c_int), ("spare", ctypes.c_int)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

@@ -33,10 +33,17 @@
 namespace g4d {
 
 constexpr uint32_t MARKER = 0xffffffffu;  // voxel without a site
-constexpr int HSLOTS = 512;               // history hash slots per star
-constexpr int HMAX = 255;                 // max history entries (hash load <= 1/2)
-constexpr int TMAX = 252;                 // max link triangles (2 * HMAX - 4)
-constexpr int TSTRIDE = 256;              // triangle slots per star in HBM
+// Two star storage classes. Every star starts in the small class; a star whose
+// history or link outgrows it (points next to a dense sheet of points, e.g. a
+// sampled sphere) moves to the large class between kernels.
+constexpr int HSLOTS = 512;               // small: history hash slots per star
+constexpr int HMAX = 255;                 // small: max history entries (hash load <= 1/2)
+constexpr int TMAX = 252;                 // small: max link triangles (2 * HMAX - 4)
+constexpr int TSTRIDE = 256;              // small: triangle slots per star in HBM
+constexpr int LHSLOTS = 2048;             // large: history hash slots
+constexpr int LHMAX = 1023;               // large: max history entries
+constexpr int LTMAX = 1020;               // large: max link triangles
+constexpr int LTSTRIDE = 1024;            // large: triangle slots in HBM
 constexpr int BUCKET_CAP = 64;            // initial candidates kept per star
 constexpr int INBOX_CAP = 64;             // insertion requests per star per round
 constexpr int MIN_WORKSET = 8;            // GDelCommon.h:49
@@ -54,17 +61,23 @@ enum : unsigned {
 };
 
 // star header flags
-enum : uint8_t { HDR_EMIT_ALL = 1, HDR_BUILT = 2 };
+enum : uint8_t { HDR_BUILT = 2 };
 
-struct StarHdr {
-    uint8_t ntri, nhist, pass, flags;
+struct __align__(8) StarHdr {
+    uint16_t ntri, nhist;
+    uint8_t pass, flags;
+    uint16_t spare;
 };
 
 // device counters (one struct in HBM, read by the host once per round)
 struct Counters {
-    int ins_count;        // stars queued for insertion
+    int ins_count;        // small stars queued for insertion
     int emit_next;        // stars queued for emission next round
     int drown_next;       // drowned items for next round
+    int ins_count_large;  // large stars queued for insertion
+    int promote_count;    // small stars that outgrew their class this round
+    int large_next;       // large-class slots handed out so far
+    int ovf_next;         // insertion requests that found a full inbox (next round)
     int overflow;         // inbox overflow happened
     unsigned err;         // ERR_* bits
     unsigned exact;       // exact predicate evaluations
@@ -82,9 +95,11 @@ __host__ __device__ inline uint32_t vx(uint32_t e) { return e & 1023u; }
 __host__ __device__ inline uint32_t vy(uint32_t e) { return (e >> 10) & 1023u; }
 __host__ __device__ inline uint32_t vz(uint32_t e) { return (e >> 20) & 1023u; }
 
-__device__ __forceinline__ uint32_t hslot0(int v) { return ((uint32_t)v * 2654435761u) >> 23; }
+// first probe of id v in a history hash of 2^LOG2 slots (multiplicative hashing)
+template <int LOG2>
+__device__ __forceinline__ uint32_t hslot0(int v) { return ((uint32_t)v * 2654435761u) >> (32 - LOG2); }
 
-// Triangle packing in HBM (8 bytes):
+// Small-class triangle packing in HBM (8 bytes):
 //   x = v0 | v1<<9 | v2<<18 | gen<<27 | kept<<31
 //   y = o0 | o1<<8 | o2<<16 | j0<<24 | j1<<26 | j2<<28
 // v* are history slots (9 bits); o* the adjacent triangle across the edge
@@ -127,6 +142,22 @@ struct Dev {
     int2* drownNext;
     int drownCap;
     Counters* ctr;
+    // large star class: lidx[s] = slot in lhh/ltri, or -1 while s is small
+    int* lidx;
+    int* lhh;              // [largeCap * LHSLOTS]
+    uint4* ltri;           // [largeCap * LTSTRIDE], packing in g4d_star.cu
+    int largeCap;
+    int* wlInsL;           // large stars with inbox requests
+    int* wlPromote;        // small stars to move to the large class
+    int anyLarge;          // some star is in the large class (else lidx is not read)
+    // requests (star, point) that found the star's inbox full: re-sent next round
+    int2* ovf;
+    int2* ovfNext;
+    int ovfCap;
+    // batches: point ranges of the clouds (sorted order), nclouds + 1 offsets;
+    // nclouds == 0 means one cloud [0, n)
+    const int* cloudOff;
+    int nclouds;
 };
 
 // ---- launchers (host) --------------------------------------------------------
@@ -144,16 +175,41 @@ void launch_gather(const Launch& L, const double* xyz, const uint32_t* vox_in, c
 void launch_colkeys(const Launch& L, const uint32_t* vox, int n, int G, uint32_t* ckey, int* cid);
 void launch_colranges(const Launch& L, const uint32_t* ckey, int n, int G, int* colStart, int* colEnd);
 
+// batches (see g4d_order.cu)
+void launch_b_order(const Launch& L, const double* xyz, int nslots, const long long* slotIn, const int* slotW,
+                    const int* slotG, unsigned long long* mm, unsigned long long* keys, int* vals, uint32_t* vox_in,
+                    long long* gidx, unsigned* err);
+void launch_b_gather(const Launch& L, const double* xyz, const long long* gidx, const uint32_t* vox_in,
+                     const int* order, const unsigned long long* skey, const int* slotW, int n, double4* P,
+                     uint32_t* vox, int* local);
+void launch_b_colkeys(const Launch& L, const uint32_t* vox, const unsigned long long* skey, const int* slotG,
+                      const long long* slotCol, int n, unsigned long long* ckey, int* cid);
+void launch_colranges_u64(const Launch& L, const unsigned long long* ckey, int n, int* colStart, int* colEnd);
+void launch_b_slot_tets(const Launch& L, const int* base, const int* slotW, int nslots, int* tc);
+void launch_b_localize(const Launch& L, const g4d_tet* in, int ntet, const unsigned long long* skey,
+                       const int* local, const int* base, const int* slotW, const long long* dst, g4d_tet* out);
+
 // pba
 void launch_pba_z(const Launch& L, const Dev& D, uint32_t* out);
 void launch_pba_y(const Launch& L, int G, const uint32_t* in, uint32_t* out);
 void launch_pba_x(const Launch& L, int G, const uint32_t* in, uint32_t* out);
 void launch_pairs(const Launch& L, const Dev& D, const uint32_t* grid);
 void launch_missing(const Launch& L, const Dev& D);
+// stacks of K grids of width G (batches; 64-bit column keys)
+void launch_pba_z_stack(const Launch& L, int G, int K, const unsigned long long* ckey, const int* cs, const int* ce,
+                        uint32_t* out);
+void launch_pba_y_stack(const Launch& L, int G, int K, const uint32_t* in, uint32_t* out);
+void launch_pba_x_stack(const Launch& L, int G, int K, const uint32_t* in, uint32_t* out);
+void launch_pairs_stack(const Launch& L, const Dev& D, const uint32_t* stack, int G, int K,
+                        const unsigned long long* ckey, const int* cid, const int* cs, const int* ce);
+void launch_missing_u64(const Launch& L, const Dev& D, const unsigned long long* mkey);
 
 // stars
 void launch_star_build(const Launch& L, const Dev& D);
 void launch_star_insert(const Launch& L, const Dev& D, int count);
+void launch_star_insert_large(const Launch& L, const Dev& D, const int* list, int count);
+void launch_promote(const Launch& L, const Dev& D, int count);
+void launch_requeue(const Launch& L, const Dev& D, int count);
 void launch_emit(const Launch& L, const Dev& D, int count);
 void launch_proof(const Launch& L, const Dev& D, int count);
 void launch_check(const Launch& L, const Dev& D, unsigned long long* bad);

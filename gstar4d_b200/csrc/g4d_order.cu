@@ -102,9 +102,10 @@ __global__ void k_colkeys(const uint32_t* __restrict__ vox, int n, int G, uint32
     }
 }
 
-__global__ void k_colranges(const uint32_t* __restrict__ ckey, int n, int* __restrict__ cs, int* __restrict__ ce) {
+template <class KeyT>
+__global__ void k_colranges(const KeyT* __restrict__ ckey, int n, int* __restrict__ cs, int* __restrict__ ce) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint32_t c = ckey[i] >> 10;
+        const KeyT c = ckey[i] >> 10;
         if (i == 0 || (ckey[i - 1] >> 10) != c) cs[c] = i;
         if (i == n - 1 || (ckey[i + 1] >> 10) != c) ce[c] = i + 1;
     }
@@ -142,6 +143,170 @@ void launch_colkeys(const Launch& L, const uint32_t* vox, int n, int G, uint32_t
 void launch_colranges(const Launch& L, const uint32_t* ckey, int n, int G, int* colStart, int* colEnd) {
     (void)G;
     k_colranges<<<blocks_for(n, 256), 256, 0, L.stream>>>(ckey, n, colStart, colEnd);
+    ++*L.launches;
+}
+
+
+// ---------------------------------------------------------------------------
+// Batches. The clouds of one pass ("slots", grouped by grid width) are sorted
+// together under 64-bit keys slot << 30 | Morton, so every cloud's points stay
+// contiguous and in its own Morton order; slotW[k] is the first sorted position
+// of slot k (and the first position of its points in the pass's input order).
+// ---------------------------------------------------------------------------
+
+// per-slot min and max over all coordinates of the cloud (one block per slot)
+__global__ void k_b_minmax(const double* __restrict__ xyz, const long long* __restrict__ slotIn,
+                           const int* __restrict__ slotW, unsigned long long* __restrict__ mm) {
+    __shared__ unsigned long long slo[32], shi[32];
+    const int k = blockIdx.x;
+    const long long m = 3LL * (slotW[k + 1] - slotW[k]);
+    const double* p = xyz + 3 * slotIn[k];
+    unsigned long long lo = ~0ull, hi = 0ull;
+    for (long long i = threadIdx.x; i < m; i += blockDim.x) {
+        const unsigned long long v = dkey(p[i]);
+        lo = v < lo ? v : lo;
+        hi = v > hi ? v : hi;
+    }
+    for (int o = 16; o; o >>= 1) {
+        const unsigned long long a = __shfl_xor_sync(0xffffffffu, lo, o);
+        const unsigned long long b = __shfl_xor_sync(0xffffffffu, hi, o);
+        lo = a < lo ? a : lo;
+        hi = b > hi ? b : hi;
+    }
+    if ((threadIdx.x & 31) == 0) { slo[threadIdx.x >> 5] = lo; shi[threadIdx.x >> 5] = hi; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+            lo = slo[w] < lo ? slo[w] : lo;
+            hi = shi[w] > hi ? shi[w] : hi;
+        }
+        mm[2 * k] = lo;
+        mm[2 * k + 1] = hi;
+    }
+}
+
+// per-slot scaling (the same arithmetic as k_scale_morton), 64-bit sort keys
+__global__ void k_b_scale(const double* __restrict__ xyz, const long long* __restrict__ slotIn,
+                          const int* __restrict__ slotW, const int* __restrict__ slotG,
+                          const unsigned long long* __restrict__ mm, unsigned long long* __restrict__ keys,
+                          int* __restrict__ vals, uint32_t* __restrict__ vox_in, long long* __restrict__ gidx,
+                          unsigned* err) {
+    const int k = blockIdx.x;
+    const int w0 = slotW[k], n = slotW[k + 1] - w0, G = slotG[k];
+    const long long in0 = slotIn[k];
+    const double mn = dkey_inv(mm[2 * k]);
+    const double rng = __dsub_rn(dkey_inv(mm[2 * k + 1]), mn);
+    const double g3 = (double)(G - 3);
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        const long long i = in0 + j;
+        uint32_t q[3];
+        for (int c = 0; c < 3; ++c) {
+            double t = __dsub_rn(xyz[3 * i + c], mn);
+            t = __dmul_rn(g3, t);
+            t = __ddiv_rn(t, rng);
+            t = __dadd_rn(t, 1.0);
+            int v = (int)t;
+            if (!(t >= 1.0) || v > G - 2) {
+                atomicOr(err, 0x100u);
+                v = v < 1 ? 1 : (v > G - 2 ? G - 2 : v);
+            }
+            q[c] = (uint32_t)v;
+        }
+        const int w = w0 + j;
+        keys[w] = ((unsigned long long)k << 30) | spread10(q[0]) | (spread10(q[1]) << 1) | (spread10(q[2]) << 2);
+        vals[w] = w;
+        vox_in[w] = enc_vox(q[0], q[1], q[2]);
+        gidx[w] = i;
+    }
+}
+
+// sorted layout: coordinates, voxels, cloud-local input index of every point
+__global__ void k_b_gather(const double* __restrict__ xyz, const long long* __restrict__ gidx,
+                           const uint32_t* __restrict__ vox_in, const int* __restrict__ order,
+                           const unsigned long long* __restrict__ skey, const int* __restrict__ slotW, int n,
+                           double4* __restrict__ P, uint32_t* __restrict__ vox, int* __restrict__ local) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int w = order[i];
+        const long long g = gidx[w];
+        P[i] = make_double4(xyz[3 * g], xyz[3 * g + 1], xyz[3 * g + 2], 0.0);
+        vox[i] = vox_in[w];
+        local[i] = w - slotW[(int)(skey[i] >> 30)];
+    }
+}
+
+// column keys: (column of the slot's grid in the stacked column index) << 10 | z
+__global__ void k_b_colkeys(const uint32_t* __restrict__ vox, const unsigned long long* __restrict__ skey,
+                            const int* __restrict__ slotG, const long long* __restrict__ slotCol, int n,
+                            unsigned long long* __restrict__ ckey, int* __restrict__ cid) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int k = (int)(skey[i] >> 30);
+        const uint32_t e = vox[i];
+        const unsigned long long col = (unsigned long long)slotCol[k] + (unsigned long long)vy(e) * slotG[k] + vx(e);
+        ckey[i] = (col << 10) | vz(e);
+        cid[i] = i;
+    }
+}
+
+// tetrahedra per slot
+__global__ void k_b_slot_tets(const int* __restrict__ base, const int* __restrict__ slotW, int nslots,
+                              int* __restrict__ tc) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nslots; k += gridDim.x * blockDim.x)
+        tc[k] = base[slotW[k + 1]] - base[slotW[k]];
+}
+
+// cloud-local tetrahedra: point ids -> the cloud's input indices, neighbour ids
+// -> the cloud's own tetrahedron numbering, written at the cloud's output offset
+__global__ void k_b_localize(const g4d_tet* __restrict__ in, int ntet, const unsigned long long* __restrict__ skey,
+                             const int* __restrict__ local, const int* __restrict__ base,
+                             const int* __restrict__ slotW, const long long* __restrict__ dst,
+                             g4d_tet* __restrict__ out) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntet; t += gridDim.x * blockDim.x) {
+        g4d_tet T = in[t];
+        const int k = (int)(skey[T.v[3]] >> 30);
+        const int tb = base[slotW[k]];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            T.v[i] = local[T.v[i]];
+            T.opp[i] = T.opp[i] >= 0 ? T.opp[i] - tb : -1;
+        }
+        out[dst[k] + (t - tb)] = T;
+    }
+}
+
+void launch_b_order(const Launch& L, const double* xyz, int nslots, const long long* slotIn, const int* slotW,
+                    const int* slotG, unsigned long long* mm, unsigned long long* keys, int* vals, uint32_t* vox_in,
+                    long long* gidx, unsigned* err) {
+    k_b_minmax<<<nslots, 256, 0, L.stream>>>(xyz, slotIn, slotW, mm);
+    k_b_scale<<<nslots, 256, 0, L.stream>>>(xyz, slotIn, slotW, slotG, mm, keys, vals, vox_in, gidx, err);
+    *L.launches += 2;
+}
+
+void launch_b_gather(const Launch& L, const double* xyz, const long long* gidx, const uint32_t* vox_in,
+                     const int* order, const unsigned long long* skey, const int* slotW, int n, double4* P,
+                     uint32_t* vox, int* local) {
+    k_b_gather<<<blocks_for(n, 256), 256, 0, L.stream>>>(xyz, gidx, vox_in, order, skey, slotW, n, P, vox, local);
+    ++*L.launches;
+}
+
+void launch_b_colkeys(const Launch& L, const uint32_t* vox, const unsigned long long* skey, const int* slotG,
+                      const long long* slotCol, int n, unsigned long long* ckey, int* cid) {
+    k_b_colkeys<<<blocks_for(n, 256), 256, 0, L.stream>>>(vox, skey, slotG, slotCol, n, ckey, cid);
+    ++*L.launches;
+}
+
+void launch_colranges_u64(const Launch& L, const unsigned long long* ckey, int n, int* colStart, int* colEnd) {
+    k_colranges<<<blocks_for(n, 256), 256, 0, L.stream>>>(ckey, n, colStart, colEnd);
+    ++*L.launches;
+}
+
+void launch_b_slot_tets(const Launch& L, const int* base, const int* slotW, int nslots, int* tc) {
+    k_b_slot_tets<<<blocks_for(nslots, 256), 256, 0, L.stream>>>(base, slotW, nslots, tc);
+    ++*L.launches;
+}
+
+void launch_b_localize(const Launch& L, const g4d_tet* in, int ntet, const unsigned long long* skey,
+                       const int* local, const int* base, const int* slotW, const long long* dst, g4d_tet* out) {
+    k_b_localize<<<blocks_for(ntet, 256), 256, 0, L.stream>>>(in, ntet, skey, local, base, slotW, dst, out);
     ++*L.launches;
 }
 

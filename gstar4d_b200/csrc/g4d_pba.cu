@@ -14,20 +14,26 @@
 //   x: same with G x TY contiguous rows (no transposes).
 // Sites stay encoded as voxel coordinates; they become point ids only for the
 // emitted pairs (a lookup in the column-sorted site list).
+//
+// Batches: the grids of all clouds with the same G are stacked (grid k of the
+// stack at offset k*G^3, its columns at k*G^2 in the column index), and each
+// kernel takes the stack depth K as its last grid dimension, so one launch per
+// grid size serves every cloud of that size. One cloud is a stack of depth 1.
 #include "g4d_internal.cuh"
 
 namespace g4d {
 
-__global__ void __launch_bounds__(128) k_pba_z(int G, const uint32_t* __restrict__ ckey, const int* __restrict__ cs,
+template <class KeyT>
+__global__ void __launch_bounds__(128) k_pba_z(int G, const KeyT* __restrict__ ckey, const int* __restrict__ cs,
                                                const int* __restrict__ ce, uint32_t* __restrict__ out) {
     const int x = blockIdx.x * 32 + threadIdx.x;
     const int y = blockIdx.y * 4 + threadIdx.y;
     if (x >= G || y >= G) return;
-    const int c = y * G + x;
+    const size_t plane = (size_t)G * G;
+    const size_t c = (size_t)blockIdx.z * plane + (size_t)y * G + x;
     int i = cs[c];
     const int e = ce[c];
-    const size_t plane = (size_t)G * G;
-    uint32_t* o = out + (size_t)y * G + x;
+    uint32_t* o = out + (size_t)blockIdx.z * plane * G + (size_t)y * G + x;
     if (i >= e) {
         for (int z = 0; z < G; ++z) o[z * plane] = MARKER;
         return;
@@ -57,7 +63,7 @@ __global__ void __launch_bounds__(256) k_pba_y(int G, const uint32_t* __restrict
     uint32_t* res = smem_pba + (size_t)TX * (G + 1);  // [G][TX+1]
     const int x0 = blockIdx.x * TX;
     const int z = blockIdx.y;
-    const size_t zoff = (size_t)z * G * G;
+    const size_t zoff = ((size_t)blockIdx.z * G + z) * G * G;
     const int total = G * TX;
     for (int k = threadIdx.x; k < total; k += blockDim.x) {
         const int yy = k / TX, xx = k % TX;
@@ -105,7 +111,7 @@ __global__ void __launch_bounds__(256) k_pba_x(int G, const uint32_t* __restrict
     extern __shared__ uint32_t tile[];
     const int y0 = blockIdx.x * TY;
     const int z = blockIdx.y;
-    const size_t base = (size_t)z * G * G + (size_t)y0 * G;
+    const size_t base = ((size_t)blockIdx.z * G + z) * G * G + (size_t)y0 * G;
     const int total = G * TY;
     const uint4* in4 = reinterpret_cast<const uint4*>(in + base);
     uint4* t4 = reinterpret_cast<uint4*>(tile);
@@ -142,12 +148,23 @@ __global__ void __launch_bounds__(256) k_pba_x(int G, const uint32_t* __restrict
     }
 }
 
+// column-sorted sites of one grid of a stack
+template <class KeyT>
+struct Cols {
+    const KeyT* key;   // (column << 10) | z, sorted
+    const int* cid;    // point id of each key
+    const int* start;  // first key of each column of this grid
+    const int* end;
+    int G;
+};
+
 // site (packed voxel) -> point id of the voxel's leader (smallest Morton index)
-__device__ __forceinline__ int site_to_id(const Dev& D, uint32_t e) {
-    const int c = (int)(vy(e) * (uint32_t)D.G + vx(e));
+template <class KeyT>
+__device__ __forceinline__ int site_to_id(const Cols<KeyT>& C, uint32_t e) {
+    const int c = (int)(vy(e) * (uint32_t)C.G + vx(e));
     const uint32_t z = vz(e);
-    for (int j = D.colStart[c], je = D.colEnd[c]; j < je; ++j)
-        if ((D.ckey[j] & 1023u) == z) return D.cid[j];
+    for (int j = C.start[c], je = C.end[c]; j < je; ++j)
+        if ((uint32_t)(C.key[j] & 1023u) == z) return C.cid[j];
     return -1;
 }
 
@@ -160,7 +177,9 @@ constexpr int PAIR_HASH = 4096;
 constexpr int PAIR_PROBES = 32;
 constexpr int PAIR_ZC = 16;
 
-__device__ __forceinline__ void pair_hash_insert(unsigned long long* hs, unsigned long long key, const Dev& D) {
+template <class KeyT>
+__device__ __forceinline__ void pair_hash_insert(unsigned long long* hs, unsigned long long key, const Dev& D,
+                                                 const Cols<KeyT>& C) {
     unsigned h = (unsigned)((key * 0x9E3779B97F4A7C15ull) >> 52) & (PAIR_HASH - 1);
     for (int probe = 0; probe < PAIR_PROBES; ++probe) {
         const unsigned long long old = atomicCAS(&hs[h], ~0ull, key);
@@ -169,7 +188,7 @@ __device__ __forceinline__ void pair_hash_insert(unsigned long long* hs, unsigne
     }
     // crowded table (dense regions hold thousands of pairs per block): emit
     // directly instead of probing further
-    const int ia = site_to_id(D, (uint32_t)(key >> 32)), ib = site_to_id(D, (uint32_t)key);
+    const int ia = site_to_id(C, (uint32_t)(key >> 32)), ib = site_to_id(C, (uint32_t)key);
     if (ia >= 0 && ib >= 0) { push_bucket(D, ia, ib); push_bucket(D, ib, ia); }
 }
 
@@ -180,16 +199,21 @@ __device__ __forceinline__ void pair_hash_insert(unsigned long long* hs, unsigne
 // keeping the previous voxel plane in registers (4 new loads per cube,
 // coalesced over x); a per-thread cache of the last pairs and a block-local
 // hash remove duplicates before the per-star scatter.
-__global__ void __launch_bounds__(128) k_pairs(Dev D, const uint32_t* __restrict__ grid) {
+template <class KeyT>
+__global__ void __launch_bounds__(128) k_pairs(Dev D, const uint32_t* __restrict__ stack, Cols<KeyT> C, int nzc) {
     __shared__ unsigned long long hs[PAIR_HASH];
-    const int G = D.G;
+    const int G = C.G;
     const int tid = threadIdx.y * 32 + threadIdx.x;
     for (int k = tid; k < PAIR_HASH; k += 128) hs[k] = ~0ull;
     __syncthreads();
     const int x = blockIdx.x * 32 + threadIdx.x;
     const int y = blockIdx.y * 4 + threadIdx.y;
-    const int z0 = blockIdx.z * PAIR_ZC;
+    const int kk = blockIdx.z / nzc;  // grid of the stack
+    const int z0 = (blockIdx.z - kk * nzc) * PAIR_ZC;
     const size_t plane = (size_t)G * G;
+    const uint32_t* grid = stack + (size_t)kk * plane * G;
+    C.start += (size_t)kk * plane;
+    C.end += (size_t)kk * plane;
     const int lane = threadIdx.x;
     // every lane of the warp walks the same z range so the warp collectives
     // below stay converged; lanes past the grid edge carry no pairs
@@ -229,7 +253,7 @@ __global__ void __launch_bounds__(128) k_pairs(Dev D, const uint32_t* __restrict
                 }
                 // lanes holding the same pair elect one inserter
                 const unsigned grp = __match_any_sync(0xffffffffu, key);
-                if (key != ~0ull && lane == __ffs(grp) - 1) pair_hash_insert(hs, key, D);
+                if (key != ~0ull && lane == __ffs(grp) - 1) pair_hash_insert(hs, key, D, C);
             }
             a0 = b0; a1 = b1; a2 = b2; a3 = b3;
         }
@@ -238,7 +262,7 @@ __global__ void __launch_bounds__(128) k_pairs(Dev D, const uint32_t* __restrict
     for (int k = tid; k < PAIR_HASH; k += 128) {
         const unsigned long long key = hs[k];
         if (key == ~0ull) continue;
-        const int ia = site_to_id(D, (uint32_t)(key >> 32)), ib = site_to_id(D, (uint32_t)key);
+        const int ia = site_to_id(C, (uint32_t)(key >> 32)), ib = site_to_id(C, (uint32_t)key);
         if (ia >= 0 && ib >= 0) {
             push_bucket(D, ia, ib);
             push_bucket(D, ib, ia);
@@ -248,24 +272,34 @@ __global__ void __launch_bounds__(128) k_pairs(Dev D, const uint32_t* __restrict
 
 // Points that share a voxel with a smaller Morton index are absent from the
 // digital diagram; each is paired with its voxel's leader (GDelKernels.cu:109-135).
-__global__ void k_missing(Dev D) {
+template <class KeyT>
+__global__ void k_missing(Dev D, const KeyT* __restrict__ mkey) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < D.n; i += gridDim.x * blockDim.x) {
-        const uint32_t k = D.mkey[i];
-        if (i == 0 || D.mkey[i - 1] != k) continue;
+        const KeyT k = mkey[i];
+        if (i == 0 || mkey[i - 1] != k) continue;
         int j = i - 1;
-        while (j > 0 && D.mkey[j - 1] == k) --j;
+        while (j > 0 && mkey[j - 1] == k) --j;
         push_bucket(D, i, j);
         push_bucket(D, j, i);
     }
 }
 
 void launch_pba_z(const Launch& L, const Dev& D, uint32_t* out) {
-    dim3 b(32, 4), g((D.G + 31) / 32, (D.G + 3) / 4);
+    dim3 b(32, 4), g((D.G + 31) / 32, (D.G + 3) / 4, 1);
     k_pba_z<<<g, b, 0, L.stream>>>(D.G, D.ckey, D.colStart, D.colEnd, out);
     ++*L.launches;
 }
 
-void launch_pba_y(const Launch& L, int G, const uint32_t* in, uint32_t* out) {
+void launch_pba_z_stack(const Launch& L, int G, int K, const unsigned long long* ckey, const int* cs, const int* ce,
+                        uint32_t* out) {
+    dim3 b(32, 4), g((G + 31) / 32, (G + 3) / 4, K);
+    k_pba_z<<<g, b, 0, L.stream>>>(G, ckey, cs, ce, out);
+    ++*L.launches;
+}
+
+void launch_pba_y(const Launch& L, int G, const uint32_t* in, uint32_t* out) { launch_pba_y_stack(L, G, 1, in, out); }
+
+void launch_pba_y_stack(const Launch& L, int G, int K, const uint32_t* in, uint32_t* out) {
     // two tiles of TX*G voxels: 64 KB for G >= 256
     const int TX = G >= 1024 ? 8 : (G >= 512 ? 16 : 32);
     const size_t sm = ((size_t)TX * (G + 1) + (size_t)G * (TX + 1)) * 4;
@@ -273,7 +307,7 @@ void launch_pba_y(const Launch& L, int G, const uint32_t* in, uint32_t* out) {
 #define G4D_Y(T)                                                                                  \
     case T:                                                                                       \
         cudaFuncSetAttribute(k_pba_y<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm); \
-        k_pba_y<T><<<dim3(G / T, G), 256, sm, L.stream>>>(G, in, out);                            \
+        k_pba_y<T><<<dim3(G / T, G, K), 256, sm, L.stream>>>(G, in, out);                         \
         break;
         G4D_Y(8) G4D_Y(16) G4D_Y(32)
 #undef G4D_Y
@@ -282,7 +316,9 @@ void launch_pba_y(const Launch& L, int G, const uint32_t* in, uint32_t* out) {
     ++*L.launches;
 }
 
-void launch_pba_x(const Launch& L, int G, const uint32_t* in, uint32_t* out) {
+void launch_pba_x(const Launch& L, int G, const uint32_t* in, uint32_t* out) { launch_pba_x_stack(L, G, 1, in, out); }
+
+void launch_pba_x_stack(const Launch& L, int G, int K, const uint32_t* in, uint32_t* out) {
     // TY rows of G voxels: 32 KB of shared memory per block
     const int TY = G >= 1024 ? 8 : (G >= 512 ? 16 : (G >= 256 ? 32 : (8192 / G < G ? 8192 / G : G)));
     const size_t sm = (size_t)G * TY * 4;
@@ -290,7 +326,7 @@ void launch_pba_x(const Launch& L, int G, const uint32_t* in, uint32_t* out) {
 #define G4D_X(T)                                                                                   \
     case T:                                                                                        \
         cudaFuncSetAttribute(k_pba_x<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);  \
-        k_pba_x<T><<<dim3(G / T, G), 256, sm, L.stream>>>(G, in, out);                             \
+        k_pba_x<T><<<dim3(G / T, G, K), 256, sm, L.stream>>>(G, in, out);                          \
         break;
         G4D_X(8) G4D_X(16) G4D_X(32) G4D_X(64) G4D_X(128) G4D_X(256)
 #undef G4D_X
@@ -301,15 +337,31 @@ void launch_pba_x(const Launch& L, int G, const uint32_t* in, uint32_t* out) {
 
 void launch_pairs(const Launch& L, const Dev& D, const uint32_t* grid) {
     const int G = D.G;
-    dim3 b(32, 4), g((G - 1 + 31) / 32, (G - 1 + 3) / 4, (G - 1 + PAIR_ZC - 1) / PAIR_ZC);
-    k_pairs<<<g, b, 0, L.stream>>>(D, grid);
+    const int nzc = (G - 1 + PAIR_ZC - 1) / PAIR_ZC;
+    dim3 b(32, 4), g((G - 1 + 31) / 32, (G - 1 + 3) / 4, nzc);
+    k_pairs<<<g, b, 0, L.stream>>>(D, grid, Cols<uint32_t>{D.ckey, D.cid, D.colStart, D.colEnd, G}, nzc);
+    ++*L.launches;
+}
+
+void launch_pairs_stack(const Launch& L, const Dev& D, const uint32_t* stack, int G, int K,
+                        const unsigned long long* ckey, const int* cid, const int* cs, const int* ce) {
+    const int nzc = (G - 1 + PAIR_ZC - 1) / PAIR_ZC;
+    dim3 b(32, 4), g((G - 1 + 31) / 32, (G - 1 + 3) / 4, nzc * K);
+    k_pairs<<<g, b, 0, L.stream>>>(D, stack, Cols<unsigned long long>{ckey, cid, cs, ce, G}, nzc);
     ++*L.launches;
 }
 
 void launch_missing(const Launch& L, const Dev& D) {
     int blocks = (D.n + 255) / 256;
     if (blocks > 148 * 16) blocks = 148 * 16;
-    k_missing<<<blocks, 256, 0, L.stream>>>(D);
+    k_missing<<<blocks, 256, 0, L.stream>>>(D, D.mkey);
+    ++*L.launches;
+}
+
+void launch_missing_u64(const Launch& L, const Dev& D, const unsigned long long* mkey) {
+    int blocks = (D.n + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    k_missing<<<blocks, 256, 0, L.stream>>>(D, mkey);
     ++*L.launches;
 }
 

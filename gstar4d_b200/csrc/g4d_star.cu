@@ -11,6 +11,14 @@
 // writes the star back once. Between rounds, emission (GDelKernels.cu:818-939)
 // and containment proofs (GDelPredKernels.cu:427-538) queue insertions into
 // per-star inboxes; the loop ends when no star receives a new point.
+//
+// Storage classes. The reference grows each star's triangle array on demand
+// (GDelData.cu:306-340). Here a star lives in a fixed small slot (255 history
+// points, 252 triangles, 4 KB in HBM, 16 KB of shared memory while a warp works
+// on it) that fits nearly every star; a star that outgrows it during a round is
+// left untouched, its inbox kept, and k_promote copies it to a large slot
+// (1023 points, 1020 triangles) before the large-class kernel replays the
+// round's insertions for it. lidx[s] says which class holds star s.
 #include "g4d_internal.cuh"
 #include "g4d_predicates.cuh"
 
@@ -18,31 +26,174 @@ namespace g4d {
 
 constexpr int WARPS_PER_BLOCK = 4;
 
-// Per-warp shared-memory image of one star (about 16 KB).
+// ---------------------------------------------------------------------------
+// storage classes
+// ---------------------------------------------------------------------------
+
+struct SmallStar {
+    static constexpr int LOG2_HS = 9, HS = HSLOTS, HM = HMAX, TM = TMAX, TS = TSTRIDE;
+    static constexpr int WARPS = WARPS_PER_BLOCK, MINB = 3;
+    static constexpr bool LARGE = false;
+    using Idx = uint8_t;   // triangle index and coordinate-cache index
+    using Rec = uint32_t;  // hole boundary edge: u | w<<9 | o<<18 | oj<<26
+    using Tri = uint2;     // packing in g4d_internal.cuh
+    __device__ static Rec rec(int u, int w, int o, int oj) {
+        return (uint32_t)u | ((uint32_t)w << 9) | ((uint32_t)o << 18) | ((uint32_t)oj << 26);
+    }
+    __device__ static int rec_u(Rec e) { return (int)(e & 511u); }
+    __device__ static int rec_w(Rec e) { return (int)((e >> 9) & 511u); }
+    __device__ static int rec_o(Rec e) { return (int)((e >> 18) & 255u); }
+    __device__ static int rec_oj(Rec e) { return (int)((e >> 26) & 3u); }
+    __device__ static int tv(Tri T, int i) { return tri_v(T, i); }
+    __device__ static int to(Tri T, int i) { return tri_o(T, i); }
+    __device__ static int tj(Tri T, int i) { return tri_j(T, i); }
+    __device__ static int gen(Tri T) { return tri_gen(T); }
+    __device__ static bool kept(Tri T) { return (T.x & TRI_KEPT) != 0; }
+    __device__ static Tri pack(int v0, int v1, int v2, int g, int o0, int o1, int o2, int j0, int j1, int j2) {
+        return tri_pack(v0, v1, v2, g, o0, o1, o2, j0, j1, j2);
+    }
+    __device__ static int* hash(const Dev& D, int s) { return D.hh + (size_t)s * HS; }
+    __device__ static Tri* tris(const Dev& D, int s) { return D.tri + (size_t)s * TS; }
+};
+
+// Large-class triangle packing in HBM (16 bytes):
+//   x = v0 | v1<<16, y = v2 | gen<<16 | kept<<31, z = o0 | o1<<16,
+//   w = o2 | j0<<16 | j1<<18 | j2<<20
+struct LargeStar {
+    static constexpr int LOG2_HS = 11, HS = LHSLOTS, HM = LHMAX, TM = LTMAX, TS = LTSTRIDE;
+    static constexpr int WARPS = 1, MINB = 2;  // about 80 KB of shared memory per warp
+    static constexpr bool LARGE = true;
+    using Idx = uint16_t;
+    using Rec = unsigned long long;  // u | w<<11 | o<<22 | oj<<32
+    using Tri = uint4;
+    __device__ static Rec rec(int u, int w, int o, int oj) {
+        return (Rec)u | ((Rec)w << 11) | ((Rec)o << 22) | ((Rec)oj << 32);
+    }
+    __device__ static int rec_u(Rec e) { return (int)(e & 2047u); }
+    __device__ static int rec_w(Rec e) { return (int)((e >> 11) & 2047u); }
+    __device__ static int rec_o(Rec e) { return (int)((e >> 22) & 1023u); }
+    __device__ static int rec_oj(Rec e) { return (int)((e >> 32) & 3u); }
+    __device__ static int tv(Tri T, int i) {
+        return (int)(i == 0 ? (T.x & 0xffffu) : (i == 1 ? (T.x >> 16) : (T.y & 0xffffu)));
+    }
+    __device__ static int to(Tri T, int i) {
+        return (int)(i == 0 ? (T.z & 0xffffu) : (i == 1 ? (T.z >> 16) : (T.w & 0xffffu)));
+    }
+    __device__ static int tj(Tri T, int i) { return (int)((T.w >> (16 + 2 * i)) & 3u); }
+    __device__ static int gen(Tri T) { return (int)((T.y >> 16) & 15u); }
+    __device__ static bool kept(Tri T) { return (T.y & 0x80000000u) != 0; }
+    __device__ static Tri pack(int v0, int v1, int v2, int g, int o0, int o1, int o2, int j0, int j1, int j2) {
+        uint4 T;
+        T.x = (uint32_t)v0 | ((uint32_t)v1 << 16);
+        T.y = (uint32_t)v2 | ((uint32_t)(g & 15) << 16);
+        T.z = (uint32_t)o0 | ((uint32_t)o1 << 16);
+        T.w = (uint32_t)o2 | ((uint32_t)j0 << 16) | ((uint32_t)j1 << 18) | ((uint32_t)j2 << 20);
+        return T;
+    }
+    __device__ static int* hash(const Dev& D, int s) { return D.lhh + (size_t)D.lidx[s] * HS; }
+    __device__ static Tri* tris(const Dev& D, int s) { return D.ltri + (size_t)D.lidx[s] * TS; }
+};
+
+// Per-warp shared-memory image of one star (16 KB small, 80 KB large).
+template <class C>
 struct WS {
-    int hh[HSLOTS];                // history hash: point id | link bit, HEMPTY when free
-    uint8_t cix[HSLOTS];           // slot -> index into the coordinate cache
-    double cx[HMAX + 1], cy[HMAX + 1], cz[HMAX + 1];
-    uint16_t tv[3][TSTRIDE];       // triangle vertices (history slots)
-    uint8_t to[3][TSTRIDE];        // neighbour across the edge opposite each vertex
-    uint8_t tj[3][TSTRIDE];        // position of the shared edge inside that neighbour
-    uint8_t tf[TSTRIDE];           // bit 7 alive, bits 0..3 creation pass
-    uint8_t efrom[HSLOTS], eto[HSLOTS];
-    uint32_t erec[TSTRIDE];        // hole boundary edges
-    uint8_t blist[TSTRIDE];        // beneath triangles in index order / compaction map
-    uint8_t fstack[TSTRIDE];       // free triangle slots
-    uint16_t order[HMAX + 1];      // insertion order (slots)
-    float okey[HMAX + 1];
-    uint32_t bmask[TSTRIDE / 32];
-    uint32_t wasLink[HSLOTS / 32], insMask[HSLOTS / 32];
+    using Idx = typename C::Idx;
+    int hh[C::HS];                 // history hash: point id | link bit, HEMPTY when free
+    Idx cix[C::HS];                // slot -> index into the coordinate cache
+    double cx[C::HM + 1], cy[C::HM + 1], cz[C::HM + 1];
+    uint16_t tv[3][C::TS];         // triangle vertices (history slots)
+    Idx to[3][C::TS];              // neighbour across the edge opposite each vertex
+    uint8_t tj[3][C::TS];          // position of the shared edge inside that neighbour
+    uint8_t tf[C::TS];             // bit 7 alive, bits 0..3 creation pass
+    Idx efrom[C::HS], eto[C::HS];
+    typename C::Rec erec[C::TS];   // hole boundary edges
+    Idx blist[C::TS];              // beneath triangles in index order / compaction map
+    Idx fstack[C::TS];             // free triangle slots
+    uint16_t order[C::HM + 1];     // insertion order (slots)
+    float okey[C::HM + 1];
+    uint32_t bmask[C::TS / 32];
+    uint32_t wasLink[C::HS / 32], insMask[C::HS / 32];
     int nedge, nfree, ntri, nins, nhist, ncoord;
 };
 
-__device__ __forceinline__ double3 wpt(const WS& S, int slot) {
+// Read-only view of any star, whichever class holds it (cross-star lookups).
+struct StarView {
+    const int* hh;
+    const void* tri;
+    bool large;
+};
+
+struct TriU {
+    int v[3], o[3], j[3];
+    int gen;
+    bool kept;
+};
+
+__device__ __forceinline__ StarView star_view(const Dev& D, int s) {
+    const int li = D.anyLarge ? D.lidx[s] : -1;
+    StarView V;
+    V.large = li >= 0;
+    if (!V.large) {
+        V.hh = D.hh + (size_t)s * HSLOTS;
+        V.tri = D.tri + (size_t)s * TSTRIDE;
+    } else {
+        V.hh = D.lhh + (size_t)li * LHSLOTS;
+        V.tri = D.ltri + (size_t)li * LTSTRIDE;
+    }
+    return V;
+}
+
+__device__ __forceinline__ TriU tri_get(const StarView& V, int t) {
+    TriU r;
+    if (!V.large) {
+        const uint2 T = static_cast<const uint2*>(V.tri)[t];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) { r.v[i] = SmallStar::tv(T, i); r.o[i] = SmallStar::to(T, i); r.j[i] = SmallStar::tj(T, i); }
+        r.gen = SmallStar::gen(T);
+        r.kept = SmallStar::kept(T);
+    } else {
+        const uint4 T = static_cast<const uint4*>(V.tri)[t];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) { r.v[i] = LargeStar::tv(T, i); r.o[i] = LargeStar::to(T, i); r.j[i] = LargeStar::tj(T, i); }
+        r.gen = LargeStar::gen(T);
+        r.kept = LargeStar::kept(T);
+    }
+    return r;
+}
+
+__device__ __forceinline__ bool tri_kept(const StarView& V, int t) {
+    return !V.large ? (static_cast<const uint2*>(V.tri)[t].x >> 31) != 0
+                    : (static_cast<const uint4*>(V.tri)[t].y >> 31) != 0;
+}
+
+__device__ __forceinline__ void tri_set_kept(const StarView& V, int t, bool keep) {
+    uint32_t* w = !V.large ? &const_cast<uint2*>(static_cast<const uint2*>(V.tri))[t].x
+                           : &const_cast<uint4*>(static_cast<const uint4*>(V.tri))[t].y;
+    const uint32_t x = *w, nx = keep ? (x | TRI_KEPT) : (x & ~TRI_KEPT);
+    if (nx != x) *w = nx;
+}
+
+// slot of v in a star's history hash (entry in *entry), -1 if absent
+__device__ __forceinline__ int view_lookup(const StarView& V, int v, uint32_t* entry) {
+    const int log2 = V.large ? LargeStar::LOG2_HS : SmallStar::LOG2_HS;
+    const uint32_t mask = (1u << log2) - 1u;
+    uint32_t s = ((uint32_t)v * 2654435761u) >> (32 - log2);
+    for (uint32_t k = 0; k <= mask; ++k) {
+        const uint32_t e = (uint32_t)V.hh[s];
+        if ((e & HID) == (uint32_t)v) { *entry = e; return (int)s; }
+        if ((e & HID) == HEMPTY) return -1;
+        s = (s + 1) & mask;
+    }
+    return -1;
+}
+
+template <class C>
+__device__ __forceinline__ double3 wpt(const WS<C>& S, int slot) {
     const int c = S.cix[slot];
     return make_double3(S.cx[c], S.cy[c], S.cz[c]);
 }
-__device__ __forceinline__ int wid(const WS& S, int slot) { return S.hh[slot] & (int)HID; }
+template <class C>
+__device__ __forceinline__ int wid(const WS<C>& S, int slot) { return S.hh[slot] & (int)HID; }
 
 __device__ __forceinline__ bool valid_id(const Dev& D, int v) { return (unsigned)v < (unsigned)D.n; }
 
@@ -66,43 +217,41 @@ __device__ __forceinline__ double3 gpt(const Dev& D, int id) {
     return make_double3(p.x, p.y, p.z);
 }
 
+// point range [lo, hi) of the cloud that holds point s
+__device__ __forceinline__ void cloud_range(const Dev& D, int s, int* lo, int* hi) {
+    if (D.nclouds <= 0) {
+        *lo = 0;
+        *hi = D.n;
+        return;
+    }
+    int a = 0, b = D.nclouds;  // cloudOff[a] <= s < cloudOff[b]
+    while (b - a > 1) {
+        const int m = (a + b) >> 1;
+        if (D.cloudOff[m] <= s) a = m; else b = m;
+    }
+    *lo = D.cloudOff[a];
+    *hi = D.cloudOff[a + 1];
+}
+
 // cache the coordinates of the point in `slot`
-__device__ __forceinline__ void ws_cache_coords(WS& S, const Dev& D, int slot, int id) {
+template <class C>
+__device__ __forceinline__ void ws_cache_coords(WS<C>& S, const Dev& D, int slot, int id) {
     const int c = atomicAdd(&S.ncoord, 1);
-    const int cc = c < HMAX + 1 ? c : HMAX;
-    S.cix[slot] = (uint8_t)cc;
+    const int cc = c < C::HM + 1 ? c : C::HM;
+    S.cix[slot] = (typename C::Idx)cc;
     const double4 p = D.P[valid_id(D, id) ? id : 0];
     S.cx[cc] = p.x;
     S.cy[cc] = p.y;
     S.cz[cc] = p.z;
 }
 
-// membership of v in star `star` (global hash): 0 = never inserted,
-// 1 = in the history but not in the link, 2 = in the link
+// membership of v in star `star`: 0 = never inserted, 1 = in the history but
+// not in the link, 2 = in the link
 __device__ __forceinline__ int hist_state(const Dev& D, int star, int v) {
     if (!valid_id(D, star)) return 1;  // never asks for an insertion into a bad star
-    const int* h = D.hh + (size_t)star * HSLOTS;
-    uint32_t s = hslot0(v);
-    for (int k = 0; k < HSLOTS; ++k) {
-        const uint32_t e = (uint32_t)h[s];
-        if ((e & HID) == (uint32_t)v) return (e & HLINK) ? 2 : 1;
-        if ((e & HID) == HEMPTY) return 0;
-        s = (s + 1) & (HSLOTS - 1);
-    }
-    return 0;
-}
-
-// slot of v in star's global hash, -1 if absent
-__device__ __forceinline__ int hist_slot(const Dev& D, int star, int v) {
-    const int* h = D.hh + (size_t)star * HSLOTS;
-    uint32_t s = hslot0(v);
-    for (int k = 0; k < HSLOTS; ++k) {
-        const uint32_t e = (uint32_t)h[s];
-        if ((e & HID) == (uint32_t)v) return (int)s;
-        if ((e & HID) == HEMPTY) return -1;
-        s = (s + 1) & (HSLOTS - 1);
-    }
-    return -1;
+    uint32_t e = 0;
+    if (view_lookup(star_view(D, star), v, &e) < 0) return 0;
+    return (e & HLINK) ? 2 : 1;
 }
 
 __device__ __forceinline__ void push_inbox(const Dev& D, int t, int v, bool* overflow) {
@@ -117,13 +266,24 @@ __device__ __forceinline__ void push_inbox(const Dev& D, int t, int v, bool* ove
         if (((volatile const int*)box)[k] == v) return;
     const int pos = atomicAdd(&D.inboxCount[t], 1);
     if (pos == 0) {
-        const int w = atomicAdd(&D.ctr->ins_count, 1);
-        D.wlIns[w] = t;
+        if (D.anyLarge && D.lidx[t] >= 0) {
+            const int w = atomicAdd(&D.ctr->ins_count_large, 1);
+            if (w < D.largeCap) D.wlInsL[w] = t;
+            else atomicOr(&D.ctr->err, ERR_CAPACITY);
+        } else {
+            const int w = atomicAdd(&D.ctr->ins_count, 1);
+            D.wlIns[w] = t;
+        }
     }
-    if (pos < INBOX_CAP)
+    if (pos < INBOX_CAP) {
         D.inbox[(size_t)t * INBOX_CAP + pos] = v;
-    else
+    } else {
+        // the inbox is full: the request waits for the next round
         *overflow = true;
+        const int q = atomicAdd(&D.ctr->ovf_next, 1);
+        if (q < D.ovfCap) D.ovfNext[q] = make_int2(t, v);
+        else atomicOr(&D.ctr->err, ERR_DROWNCAP);
+    }
 }
 
 // --------------------------------------------------------------------------
@@ -142,13 +302,14 @@ __device__ __forceinline__ int warp_excl_scan(int v, int lane, int* total) {
 }
 
 // Insert id v into the shared history hash; returns slot, sets *fresh when new.
-__device__ __forceinline__ int ws_hash_insert(WS& S, int v, bool* fresh) {
-    uint32_t s = hslot0(v);
-    for (int k = 0; k < HSLOTS; ++k) {
+template <class C>
+__device__ __forceinline__ int ws_hash_insert(WS<C>& S, int v, bool* fresh) {
+    uint32_t s = hslot0<C::LOG2_HS>(v);
+    for (int k = 0; k < C::HS; ++k) {
         const int old = atomicCAS(&S.hh[s], (int)HEMPTY, v);
         if ((uint32_t)old == HEMPTY) { *fresh = true; return (int)s; }
         if ((old & (int)HID) == v) { *fresh = false; return (int)s; }
-        s = (s + 1) & (HSLOTS - 1);
+        s = (s + 1) & (C::HS - 1);
     }
     *fresh = false;
     return -1;
@@ -156,9 +317,12 @@ __device__ __forceinline__ int ws_hash_insert(WS& S, int v, bool* fresh) {
 
 // Insert the point in slot sp into the star held by the warp. Returns 1 when it
 // entered the link, 0 when it lies inside the star's cone (drowned), -1 on an
-// error (flag raised).
-__device__ int warp_insert(WS& S, int lane, int s, double3 ps, int sp, int gen, const PredSink& sink,
+// error (flag raised), -2 when the star's class has no room for the new
+// triangles (the caller promotes the star or reports the capacity error).
+template <class C>
+__device__ int warp_insert(WS<C>& S, int lane, int s, double3 ps, int sp, int gen, const PredSink& sink,
                            unsigned* exact) {
+    using Idx = typename C::Idx;
     unsigned* err = sink.err;
     const double3 pp = wpt(S, sp);
     const int pid = wid(S, sp);
@@ -193,30 +357,27 @@ __device__ int warp_insert(WS& S, int lane, int s, double3 ps, int sp, int gen, 
         const unsigned m = S.bmask[base >> 5];
         const int t = base + lane;
         const bool b = (m >> lane) & 1u;
-        if (b) S.blist[prefix + __popc(m & ((1u << lane) - 1u))] = (uint8_t)t;
+        if (b) S.blist[prefix + __popc(m & ((1u << lane) - 1u))] = (Idx)t;
         prefix += __popc(m);
-        uint32_t rec[3];
+        typename C::Rec rec[3];
         int ne = 0;
         if (b) {
 #pragma unroll
             for (int i = 0; i < 3; ++i) {
                 const int o = S.to[i][t];
                 const bool ob = (S.bmask[o >> 5] >> (o & 31)) & 1u;
-                if (!ob) {
-                    const int u = S.tv[(i + 1) % 3][t], w = S.tv[(i + 2) % 3][t];
-                    rec[ne++] = (uint32_t)u | ((uint32_t)w << 9) | ((uint32_t)o << 18) | ((uint32_t)S.tj[i][t] << 26);
-                }
+                if (!ob) rec[ne++] = C::rec(S.tv[(i + 1) % 3][t], S.tv[(i + 2) % 3][t], o, S.tj[i][t]);
             }
         }
         int total;
         const int start = nedge + warp_excl_scan(ne, lane, &total);
         for (int k = 0; k < ne; ++k)
-            if (start + k < TSTRIDE) S.erec[start + k] = rec[k];
+            if (start + k < C::TS) S.erec[start + k] = rec[k];
         nedge += total;
     }
     __syncwarp();
     const int B = nedge;
-    if (B > HMAX) {  // a disk's boundary visits each link vertex at most once
+    if (B > C::HM) {  // a disk's boundary visits each link vertex at most once
         if (lane == 0) {
             atomicOr(err, ERR_TOPOLOGY);
             G4D_TRACE("star %d: point %d hole boundary of %d edges\n", s, pid, B);
@@ -228,17 +389,10 @@ __device__ int warp_insert(WS& S, int lane, int s, double3 ps, int sp, int gen, 
     const int extra = B - nb;
     const int from_free = extra > 0 ? (extra < nfree ? extra : nfree) : 0;
     const int appended = extra > 0 ? extra - from_free : 0;
-    if (ntri + appended > TMAX) {
-        if (lane == 0) {
-            atomicOr(err, ERR_CAPACITY);
-            G4D_TRACE("star %d: point %d needs %d triangles (nb %d, B %d, free %d)\n", s, pid, ntri + appended, nb,
-                      B, nfree);
-        }
-        return -1;
-    }
+    if (ntri + appended > C::TM) return -2;
     for (int r = lane; r < B; r += 32) {
-        const uint32_t e = S.erec[r];
-        const int u = e & 511, w = (e >> 9) & 511;
+        const typename C::Rec e = S.erec[r];
+        const int u = C::rec_u(e), w = C::rec_w(e);
         int slot;
         if (r < nb) {
             slot = S.blist[r];
@@ -246,14 +400,14 @@ __device__ int warp_insert(WS& S, int lane, int s, double3 ps, int sp, int gen, 
             const int rr = r - nb;
             slot = rr < nfree ? S.fstack[nfree - 1 - rr] : ntri + (rr - nfree);
         }
-        S.efrom[u] = (uint8_t)slot;
-        S.eto[w] = (uint8_t)slot;
+        S.efrom[u] = (Idx)slot;
+        S.eto[w] = (Idx)slot;
     }
     __syncwarp();
     // new triangle (u, w, p) replaces the beneath triangle across the edge u->w
     for (int r = lane; r < B; r += 32) {
-        const uint32_t e = S.erec[r];
-        const int u = e & 511, w = (e >> 9) & 511, o = (e >> 18) & 255, oj = (e >> 26) & 3;
+        const typename C::Rec e = S.erec[r];
+        const int u = C::rec_u(e), w = C::rec_w(e), o = C::rec_o(e), oj = C::rec_oj(e);
         const int slot = S.efrom[u];
         S.tv[0][slot] = (uint16_t)u;
         S.tv[1][slot] = (uint16_t)w;
@@ -262,10 +416,10 @@ __device__ int warp_insert(WS& S, int lane, int s, double3 ps, int sp, int gen, 
         S.tj[0][slot] = 1;
         S.to[1][slot] = S.eto[u];    // edge (p, u): the previous boundary edge's triangle
         S.tj[1][slot] = 0;
-        S.to[2][slot] = (uint8_t)o;  // edge (u, w): the triangle outside the hole
+        S.to[2][slot] = (Idx)o;      // edge (u, w): the triangle outside the hole
         S.tj[2][slot] = (uint8_t)oj;
         if (oj < 3) {
-            S.to[oj][o] = (uint8_t)slot;
+            S.to[oj][o] = (Idx)slot;
             S.tj[oj][o] = 2;
         }
         S.tf[slot] = (uint8_t)(0x80 | gen);
@@ -275,7 +429,7 @@ __device__ int warp_insert(WS& S, int lane, int s, double3 ps, int sp, int gen, 
         for (int r = B + lane; r < nb; r += 32) {
             const int t = S.blist[r];
             S.tf[t] = 0;
-            S.fstack[nfree + (r - B)] = (uint8_t)t;
+            S.fstack[nfree + (r - B)] = (Idx)t;
         }
     }
     __syncwarp();
@@ -293,7 +447,8 @@ __device__ int warp_insert(WS& S, int lane, int s, double3 ps, int sp, int gen, 
 
 // cone of the pentachoron (l0..l3, star): the link triangles of the 4-simplex
 // (GDelPredKernels.cu:45-158), oriented so that orient4(tri, star, opposite) > 0
-__device__ void warp_cone(WS& S, int lane, int s, double3 ps, const int* l4, int gen, const PredSink& sink,
+template <class C>
+__device__ void warp_cone(WS<C>& S, int lane, int s, double3 ps, const int* l4, int gen, const PredSink& sink,
                           unsigned* exact) {
     int l[4] = {l4[0], l4[1], l4[2], l4[3]};
     const int o = orient4(wpt(S, l[0]), wpt(S, l[1]), wpt(S, l[2]), wpt(S, l[3]), ps, wid(S, l[0]), wid(S, l[1]),
@@ -305,7 +460,7 @@ __device__ void warp_cone(WS& S, int lane, int s, double3 ps, const int* l4, int
         for (int i = 0; i < 3; ++i) {
             S.tv[i][f] = (uint16_t)l[F[f][i]];
             const int b = F[f][i];  // the face omitting vertex F[f][i] shares this edge
-            S.to[i][f] = (uint8_t)b;
+            S.to[i][f] = (typename C::Idx)b;
             int j = 0;
             for (int k = 0; k < 3; ++k)
                 if (F[b][k] == f) j = k;
@@ -320,8 +475,9 @@ __device__ void warp_cone(WS& S, int lane, int s, double3 ps, const int* l4, int
     __syncwarp();
 }
 
-// sort order[0..n) by okey ascending (bitonic over a power of two <= HMAX + 1)
-__device__ void warp_sort_order(WS& S, int lane, int n) {
+// sort order[0..n) by okey ascending (bitonic over a power of two <= HM + 1)
+template <class C>
+__device__ void warp_sort_order(WS<C>& S, int lane, int n) {
     int m = 1;
     while (m < n) m <<= 1;
     for (int i = n + lane; i < m; i += 32) { S.okey[i] = 3.0e38f; S.order[i] = 0; }
@@ -344,14 +500,16 @@ __device__ void warp_sort_order(WS& S, int lane, int n) {
 }
 
 // Load star s (history, coordinates, triangles) into shared memory.
-__device__ void warp_load(WS& S, const Dev& D, int lane, int s, StarHdr h) {
+template <class C>
+__device__ void warp_load(WS<C>& S, const Dev& D, int lane, int s, StarHdr h) {
+    using Idx = typename C::Idx;
     if (lane == 0) {
         S.ncoord = 0;
         S.nins = 0;
     }
     __syncwarp();
-    const int* gh = D.hh + (size_t)s * HSLOTS;
-    for (int k = lane; k < HSLOTS; k += 32) {
+    const int* gh = C::hash(D, s);
+    for (int k = lane; k < C::HS; k += 32) {
         const int e = gh[k];
         S.hh[k] = e;
         const bool occ = (uint32_t)(e & (int)HID) != HEMPTY;
@@ -359,15 +517,16 @@ __device__ void warp_load(WS& S, const Dev& D, int lane, int s, StarHdr h) {
         const unsigned m = __ballot_sync(0xffffffffu, occ && (e & (int)HLINK) != 0);
         if (lane == 0) { S.wasLink[k >> 5] = m; S.insMask[k >> 5] = 0; }
     }
-    const uint2* gt = D.tri + (size_t)s * TSTRIDE;
+    const typename C::Tri* gt = C::tris(D, s);
     for (int t = lane; t < h.ntri; t += 32) {
-        const uint2 T = gt[t];
-        S.tv[0][t] = (uint16_t)tri_v(T, 0);
-        S.tv[1][t] = (uint16_t)tri_v(T, 1);
-        S.tv[2][t] = (uint16_t)tri_v(T, 2);
-        S.tf[t] = (uint8_t)(0x80 | tri_gen(T));
-        S.to[0][t] = (uint8_t)tri_o(T, 0); S.to[1][t] = (uint8_t)tri_o(T, 1); S.to[2][t] = (uint8_t)tri_o(T, 2);
-        S.tj[0][t] = (uint8_t)tri_j(T, 0); S.tj[1][t] = (uint8_t)tri_j(T, 1); S.tj[2][t] = (uint8_t)tri_j(T, 2);
+        const typename C::Tri T = gt[t];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            S.tv[i][t] = (uint16_t)C::tv(T, i);
+            S.to[i][t] = (Idx)C::to(T, i);
+            S.tj[i][t] = (uint8_t)C::tj(T, i);
+        }
+        S.tf[t] = (uint8_t)(0x80 | C::gen(T));
     }
     if (lane == 0) {
         S.ntri = h.ntri;
@@ -378,7 +537,9 @@ __device__ void warp_load(WS& S, const Dev& D, int lane, int s, StarHdr h) {
 }
 
 // Compact triangles, refresh link bits, report drowned points, write back.
-__device__ void warp_store(WS& S, const Dev& D, int lane, int s, int pass, bool created) {
+template <class C>
+__device__ void warp_store(WS<C>& S, const Dev& D, int lane, int s, int pass, bool created) {
+    using Idx = typename C::Idx;
     const int ntri = S.ntri;
     int nalive = 0;
     // new index of each live triangle (blist reused as the map)
@@ -386,25 +547,25 @@ __device__ void warp_store(WS& S, const Dev& D, int lane, int s, int pass, bool 
         const int t = base + lane;
         const bool al = t < ntri && (S.tf[t] & 0x80);
         const unsigned m = __ballot_sync(0xffffffffu, al);
-        if (al) S.blist[t] = (uint8_t)(nalive + __popc(m & ((1u << lane) - 1u)));
+        if (al) S.blist[t] = (Idx)(nalive + __popc(m & ((1u << lane) - 1u)));
         nalive += __popc(m);
     }
-    for (int k = lane; k < HSLOTS; k += 32) S.hh[k] &= (int)HID;
+    for (int k = lane; k < C::HS; k += 32) S.hh[k] &= (int)HID;
     __syncwarp();
     for (int t = lane; t < ntri; t += 32) {
         if (!(S.tf[t] & 0x80)) continue;
         for (int i = 0; i < 3; ++i) atomicOr(&S.hh[S.tv[i][t]], (int)HLINK);
     }
     __syncwarp();
-    uint2* gt = D.tri + (size_t)s * TSTRIDE;
+    typename C::Tri* gt = C::tris(D, s);
     for (int t = lane; t < ntri; t += 32) {
         if (!(S.tf[t] & 0x80)) continue;
-        gt[S.blist[t]] = tri_pack(S.tv[0][t], S.tv[1][t], S.tv[2][t], S.tf[t] & 15, S.blist[S.to[0][t]],
-                                  S.blist[S.to[1][t]], S.blist[S.to[2][t]], S.tj[0][t], S.tj[1][t], S.tj[2][t]);
+        gt[S.blist[t]] = C::pack(S.tv[0][t], S.tv[1][t], S.tv[2][t], S.tf[t] & 15, S.blist[S.to[0][t]],
+                                 S.blist[S.to[1][t]], S.blist[S.to[2][t]], S.tj[0][t], S.tj[1][t], S.tj[2][t]);
     }
     // drowned: linked before or inserted now, not linked after
-    int* gh = D.hh + (size_t)s * HSLOTS;
-    for (int k = lane; k < HSLOTS; k += 32) {
+    int* gh = C::hash(D, s);
+    for (int k = lane; k < C::HS; k += 32) {
         const int e = S.hh[k];
         gh[k] = e;
         const bool occupied = (uint32_t)(e & (int)HID) != HEMPTY;
@@ -424,10 +585,11 @@ __device__ void warp_store(WS& S, const Dev& D, int lane, int s, int pass, bool 
     }
     if (lane == 0) {
         StarHdr h;
-        h.ntri = (uint8_t)nalive;
-        h.nhist = (uint8_t)S.nhist;
+        h.ntri = (uint16_t)nalive;
+        h.nhist = (uint16_t)S.nhist;
         h.pass = (uint8_t)pass;
         h.flags = HDR_BUILT;
+        h.spare = 0;
         D.hdr[s] = h;
         if (created) {
             const int w = atomicAdd(&D.ctr->emit_next, 1);
@@ -438,23 +600,25 @@ __device__ void warp_store(WS& S, const Dev& D, int lane, int s, int pass, bool 
 }
 
 // --------------------------------------------------------------------------
-// build: initial star of every point from its candidate workset
+// build: initial star of every point from its candidate workset (at most
+// BUCKET_CAP + MIN_WORKSET points, so always the small class)
 // --------------------------------------------------------------------------
 
 // 3 blocks per SM: shared memory (about 65 KB per block) allows no more, and
 // this register budget (168) costs only a few hundred bytes of spills.
 __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK, 3) k_star_build(Dev D) {
     G4D_DYN_SMEM(smem_raw);
+    using C = SmallStar;
     const int lane = threadIdx.x & 31;
-    WS& S = reinterpret_cast<WS*>(smem_raw)[threadIdx.x >> 5];
+    WS<C>& S = reinterpret_cast<WS<C>*>(smem_raw)[threadIdx.x >> 5];
     const PredSink sink = sink_of(D);
     unsigned* err = sink.err;
     unsigned* exact = &D.ctr->exact;
     const int warps = gridDim.x * WARPS_PER_BLOCK;
     for (int s = blockIdx.x * WARPS_PER_BLOCK + (threadIdx.x >> 5); s < D.n; s += warps) {
         __syncwarp();  // the previous star's shared-memory reads are done
-        for (int k = lane; k < HSLOTS; k += 32) S.hh[k] = (int)HEMPTY;
-        for (int k = lane; k < HSLOTS / 32; k += 32) { S.wasLink[k] = 0; S.insMask[k] = 0; }
+        for (int k = lane; k < C::HS; k += 32) S.hh[k] = (int)HEMPTY;
+        for (int k = lane; k < C::HS / 32; k += 32) { S.wasLink[k] = 0; S.insMask[k] = 0; }
         if (lane == 0) { S.nins = 0; S.nhist = 0; S.ntri = 0; S.nfree = 0; S.ncoord = 0; }
         __syncwarp();
         const double3 ps = gpt(D, s);
@@ -474,7 +638,7 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK, 3) k_star_build(Dev D) {
         const int ncand = S.nins;
         __syncwarp();  // every lane has read the count before lane 0 may change it
         // pumping (GDelKernels.cu:370-477): fewer than MIN_WORKSET candidates borrow
-        // from their candidates' worksets, then from the first point ids
+        // from their candidates' worksets, then from the first point ids of the cloud
         if (ncand < MIN_WORKSET) {
             if (lane == 0) {
                 int have = ncand;
@@ -489,7 +653,9 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK, 3) k_star_build(Dev D) {
                         if (fresh) S.order[have++] = (uint16_t)slot;
                     }
                 }
-                for (int v = 0; v < D.n && have < MIN_WORKSET; ++v) {
+                int lo, hi;
+                cloud_range(D, s, &lo, &hi);
+                for (int v = lo; v < hi && have < MIN_WORKSET; ++v) {
                     if (v == s) continue;
                     bool fresh;
                     const int slot = ws_hash_insert(S, v, &fresh);
@@ -504,9 +670,9 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK, 3) k_star_build(Dev D) {
             __syncwarp();
         }
         const int nins = S.nins;
-        if (nins > HMAX || nins < 4) {
+        if (nins > C::HM || nins < 4) {
             if (lane == 0) {
-                atomicOr(err, nins > HMAX ? ERR_CAPACITY : ERR_TOPOLOGY);
+                atomicOr(err, nins > C::HM ? ERR_CAPACITY : ERR_TOPOLOGY);
                 G4D_TRACE("star %d: %d initial candidates\n", s, nins);
             }
             continue;
@@ -531,6 +697,7 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK, 3) k_star_build(Dev D) {
         int failed = 0;
         for (int i = 4; i < nins && !failed; ++i) {
             const int r = warp_insert(S, lane, s, ps, S.order[i], gen, sink, exact);
+            if (r == -2 && lane == 0) atomicOr(err, ERR_CAPACITY);
             failed = r < 0;
         }
         if (failed) continue;
@@ -540,20 +707,22 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK, 3) k_star_build(Dev D) {
 }
 
 // --------------------------------------------------------------------------
-// insertion round: every star with inbox requests
+// insertion round: every star with inbox requests. A small star that outgrows
+// its class keeps its inbox and joins the promotion list.
 // --------------------------------------------------------------------------
 
-__global__ void __launch_bounds__(32 * WARPS_PER_BLOCK, 3) k_star_insert(Dev D, int count) {
+template <class C>
+__global__ void __launch_bounds__(32 * C::WARPS, C::MINB) k_star_insert(Dev D, const int* list, int count) {
     G4D_DYN_SMEM(smem_raw);
     const int lane = threadIdx.x & 31;
-    WS& S = reinterpret_cast<WS*>(smem_raw)[threadIdx.x >> 5];
+    WS<C>& S = reinterpret_cast<WS<C>*>(smem_raw)[threadIdx.x >> 5];
     const PredSink sink = sink_of(D);
     unsigned* err = sink.err;
     unsigned* exact = &D.ctr->exact;
-    const int warps = gridDim.x * WARPS_PER_BLOCK;
-    for (int w = blockIdx.x * WARPS_PER_BLOCK + (threadIdx.x >> 5); w < count; w += warps) {
+    const int warps = gridDim.x * C::WARPS;
+    for (int w = blockIdx.x * C::WARPS + (threadIdx.x >> 5); w < count; w += warps) {
         __syncwarp();  // the previous item's shared-memory reads are done
-        const int s = D.wlIns[w];
+        const int s = list[w];
         const StarHdr h = D.hdr[s];
         warp_load(S, D, lane, s, h);
         const double3 ps = gpt(D, s);
@@ -561,42 +730,99 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK, 3) k_star_insert(Dev D, 
         int* box = D.inbox + (size_t)s * INBOX_CAP;
         for (int k = lane; k < ic; k += 32) {
             const int v = box[k];
-            box[k] = -1;
             if (v == s || !valid_id(D, v)) continue;
             bool fresh;
             const int slot = ws_hash_insert(S, v, &fresh);
             if (slot < 0) { atomicOr(err, ERR_CAPACITY); continue; }
             if (fresh) {
                 const int pos = atomicAdd(&S.nins, 1);
-                S.order[pos < HMAX ? pos : HMAX] = (uint16_t)slot;
+                S.order[pos < C::HM ? pos : C::HM] = (uint16_t)slot;
                 ws_cache_coords(S, D, slot, v);
                 atomicOr(&S.insMask[slot >> 5], 1u << (slot & 31));
             }
         }
         __syncwarp();
-        if (lane == 0) D.inboxCount[s] = 0;
         const int nins = S.nins;
         const int nhist0 = S.nhist;
         __syncwarp();  // all lanes read the counts before lane 0 updates them
-        if (nhist0 + nins > HMAX) {
+        bool outgrown = nhist0 + nins > C::HM;
+        int any = 0, failed = 0;
+        const int gen = (h.pass % 15) + 1;  // 1..15, differs from the stored pass
+        if (!outgrown) {
+            if (lane == 0) S.nhist = nhist0 + nins;
+            __syncwarp();
+            for (int i = 0; i < nins && !failed; ++i) {
+                const int r = warp_insert(S, lane, s, ps, S.order[i], gen, sink, exact);
+                outgrown = r == -2;
+                failed = r < 0;
+                any |= r > 0;
+            }
+        }
+        if (outgrown) {
             if (lane == 0) {
-                atomicOr(err, ERR_CAPACITY);
-                G4D_TRACE("star %d: history %d + %d exceeds %d\n", s, nhist0, nins, HMAX);
+                if (C::LARGE) {
+                    atomicOr(err, ERR_CAPACITY);
+                    G4D_TRACE("star %d: history %d + %d outgrows the large class\n", s, nhist0, nins);
+                } else {
+                    const int q = atomicAdd(&D.ctr->promote_count, 1);
+                    D.wlPromote[q] = s;
+                }
             }
             continue;
         }
-        if (lane == 0) S.nhist = nhist0 + nins;
-        __syncwarp();
-        const int gen = (h.pass % 15) + 1;  // 1..15, differs from the stored pass
-        int any = 0, failed = 0;
-        for (int i = 0; i < nins && !failed; ++i) {
-            const int r = warp_insert(S, lane, s, ps, S.order[i], gen, sink, exact);
-            failed = r < 0;
-            any |= r > 0;
-        }
         if (failed) continue;
+        for (int k = lane; k < ic; k += 32) box[k] = -1;  // the inbox is consumed
+        if (lane == 0) D.inboxCount[s] = 0;
         warp_store(S, D, lane, s, any ? gen : h.pass, any != 0);
         if (lane == 0) atomicAdd(&D.ctr->insertions, (unsigned long long)nins);
+    }
+}
+
+// --------------------------------------------------------------------------
+// promotion: copy small stars to large slots (history re-hashed into 2048
+// slots, triangle vertex slots remapped, triangles widened to 16 bytes)
+// --------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_promote(Dev D, int count) {
+    __shared__ uint16_t smap[WARPS_PER_BLOCK][HSLOTS];
+    const int lane = threadIdx.x & 31;
+    uint16_t* map = smap[threadIdx.x >> 5];
+    const int warps = gridDim.x * WARPS_PER_BLOCK;
+    for (int w = blockIdx.x * WARPS_PER_BLOCK + (threadIdx.x >> 5); w < count; w += warps) {
+        __syncwarp();
+        const int s = D.wlPromote[w];
+        int li = 0;
+        if (lane == 0) li = atomicAdd(&D.ctr->large_next, 1);
+        li = __shfl_sync(0xffffffffu, li, 0);
+        if (li >= D.largeCap) {
+            if (lane == 0) atomicOr(&D.ctr->err, ERR_CAPACITY);
+            continue;
+        }
+        int* nh = D.lhh + (size_t)li * LHSLOTS;
+        for (int k = lane; k < LHSLOTS; k += 32) nh[k] = (int)HEMPTY;
+        __syncwarp();
+        const int* oh = D.hh + (size_t)s * HSLOTS;
+        for (int k = lane; k < HSLOTS; k += 32) {
+            const int e = oh[k];
+            if ((uint32_t)(e & (int)HID) == HEMPTY) continue;
+            uint32_t slot = hslot0<LargeStar::LOG2_HS>(e & (int)HID);
+            for (int probe = 0; probe < LHSLOTS; ++probe) {
+                if (atomicCAS(&nh[slot], (int)HEMPTY, e) == (int)HEMPTY) break;
+                slot = (slot + 1) & (LHSLOTS - 1);
+            }
+            map[k] = (uint16_t)slot;
+        }
+        __syncwarp();
+        const StarHdr h = D.hdr[s];
+        const uint2* ot = D.tri + (size_t)s * TSTRIDE;
+        uint4* nt = D.ltri + (size_t)li * LTSTRIDE;
+        for (int t = lane; t < h.ntri; t += 32) {
+            const uint2 T = ot[t];
+            nt[t] = LargeStar::pack(map[tri_v(T, 0)], map[tri_v(T, 1)], map[tri_v(T, 2)], tri_gen(T), tri_o(T, 0),
+                                    tri_o(T, 1), tri_o(T, 2), tri_j(T, 0), tri_j(T, 1), tri_j(T, 2));
+        }
+        __syncwarp();
+        if (lane == 0) D.lidx[s] = li;
     }
 }
 
@@ -605,25 +831,30 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK, 3) k_star_insert(Dev D, 
 // each other (GDelKernels.cu:818-939)
 // --------------------------------------------------------------------------
 
+// history ids of star s by slot: small stars are copied to shared memory,
+// large ones are read in place
+__device__ __forceinline__ const int* stage_ids(const StarView& V, int* smem, int lane) {
+    if (V.large) return V.hh;
+    for (int k = lane; k < HSLOTS; k += 32) smem[k] = V.hh[k] & (int)HID;
+    __syncwarp();
+    return smem;
+}
+
 __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_emit(Dev D, int count) {
     __shared__ int shh[WARPS_PER_BLOCK][HSLOTS];
     const int lane = threadIdx.x & 31;
-    int* hh = shh[threadIdx.x >> 5];
     const int warps = gridDim.x * WARPS_PER_BLOCK;
     for (int w = blockIdx.x * WARPS_PER_BLOCK + (threadIdx.x >> 5); w < count; w += warps) {
         __syncwarp();  // the previous item's shared-memory reads are done
         const int s = D.wlEmit[w];
-        StarHdr h = D.hdr[s];
-        const bool all = (h.flags & HDR_EMIT_ALL) != 0;
-        const int* gh = D.hh + (size_t)s * HSLOTS;
-        for (int k = lane; k < HSLOTS; k += 32) hh[k] = gh[k] & (int)HID;
-        __syncwarp();
-        const uint2* gt = D.tri + (size_t)s * TSTRIDE;
+        const StarHdr h = D.hdr[s];
+        const StarView V = star_view(D, s);
+        const int* ids = stage_ids(V, shh[threadIdx.x >> 5], lane);
         bool ovf = false;
         for (int t = lane; t < h.ntri; t += 32) {
-            const uint2 T = gt[t];
-            if (!all && tri_gen(T) != h.pass) continue;
-            const int v[3] = {hh[tri_v(T, 0)], hh[tri_v(T, 1)], hh[tri_v(T, 2)]};
+            const TriU T = tri_get(V, t);
+            if (T.gen != h.pass) continue;
+            const int v[3] = {ids[T.v[0]] & (int)HID, ids[T.v[1]] & (int)HID, ids[T.v[2]] & (int)HID};
             for (int i = 0; i < 3; ++i) {
                 const int a = v[i], b = v[(i + 1) % 3];
                 if (a > b) continue;
@@ -635,19 +866,16 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_emit(Dev D, int count)
                 if (hist_state(D, b, a) == 0) push_inbox(D, b, a, &ovf);
             }
         }
-        const unsigned anyovf = __ballot_sync(0xffffffffu, ovf);
-        if (lane == 0) {
-            if (anyovf) {
-                h.flags |= HDR_EMIT_ALL;
-                const int q = atomicAdd(&D.ctr->emit_next, 1);
-                D.wlEmitNext[q] = s;
-                atomicOr(&D.ctr->overflow, 1);
-            } else {
-                h.flags &= ~HDR_EMIT_ALL;
-            }
-            D.hdr[s] = h;
-        }
-        __syncwarp();
+        if (__ballot_sync(0xffffffffu, ovf) && lane == 0) atomicOr(&D.ctr->overflow, 1);
+    }
+}
+
+// requests that found a full inbox last round, re-sent while still needed
+__global__ void k_requeue(Dev D, int count) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const int2 r = D.ovf[i];
+        bool ovf = false;
+        if (hist_state(D, r.x, r.y) == 0) push_inbox(D, r.x, r.y, &ovf);
     }
 }
 
@@ -658,7 +886,6 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_emit(Dev D, int count)
 __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_proof(Dev D, int count) {
     __shared__ int shh[WARPS_PER_BLOCK][HSLOTS];
     const int lane = threadIdx.x & 31;
-    int* hh = shh[threadIdx.x >> 5];
     const PredSink sink = sink_of(D);
     unsigned* err = sink.err;
     unsigned* exact = &D.ctr->exact;
@@ -672,12 +899,10 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_proof(Dev D, int count
         if (hist_state(D, v, s) != 2) continue;
         const StarHdr h = D.hdr[s];
         if (h.ntri == 0) continue;
-        const int* gh = D.hh + (size_t)s * HSLOTS;
-        for (int k = lane; k < HSLOTS; k += 32) hh[k] = gh[k] & (int)HID;
-        __syncwarp();
-        const uint2* gt = D.tri + (size_t)s * TSTRIDE;
+        const StarView V = star_view(D, s);
+        const int* ids = stage_ids(V, shh[threadIdx.x >> 5], lane);
         const double3 ps = gpt(D, s), pv = gpt(D, v);
-        const int ex = hh[tri_v(gt[0], 0)];
+        const int ex = ids[tri_get(V, 0).v[0]] & (int)HID;
         const double3 pe = gpt(D, ex);
         int found_t = 0x7fffffff;
         int pa = -1, pb = -1, pc = -1;
@@ -686,8 +911,8 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_proof(Dev D, int count
             bool ok = false;
             int a = -1, b = -1, c = -1;
             if (t < h.ntri) {
-                const uint2 T = gt[t];
-                a = hh[tri_v(T, 0)]; b = hh[tri_v(T, 1)]; c = hh[tri_v(T, 2)];
+                const TriU T = tri_get(V, t);
+                a = ids[T.v[0]] & (int)HID; b = ids[T.v[1]] & (int)HID; c = ids[T.v[2]] & (int)HID;
                 if (a != ex && b != ex && c != ex) {
                     const double3 qa = gpt(D, a), qb = gpt(D, b), qc = gpt(D, c);
                     const int o0 = orient4(ps, pv, pe, qa, qb, s, v, ex, a, b, sink, exact);
@@ -727,11 +952,7 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_proof(Dev D, int count
         const unsigned anyovf = __ballot_sync(0xffffffffu, ovf);
         if (lane == 0) {
             atomicAdd(&D.ctr->proofs_total, 1ull);
-            if (anyovf) {
-                const int q = atomicAdd(&D.ctr->drown_next, 1);
-                if (q < D.drownCap) D.drownNext[q] = item;
-                atomicOr(&D.ctr->overflow, 1);
-            }
+            if (anyovf) atomicOr(&D.ctr->overflow, 1);
         }
     }
 }
@@ -745,13 +966,14 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_proof(Dev D, int count
 // `cyclic`), or -1
 __device__ int find_tri(const Dev& D, int star, int x, int y, int z, bool cyclic) {
     if (!valid_id(D, star)) return -1;
-    const int sx = hist_slot(D, star, x), sy = hist_slot(D, star, y), sz = hist_slot(D, star, z);
+    const StarView V = star_view(D, star);
+    uint32_t e;
+    const int sx = view_lookup(V, x, &e), sy = view_lookup(V, y, &e), sz = view_lookup(V, z, &e);
     if (sx < 0 || sy < 0 || sz < 0) return -1;
     const StarHdr hd = D.hdr[star];
-    const uint2* gt = D.tri + (size_t)star * TSTRIDE;
     for (int t = 0; t < hd.ntri; ++t) {
-        const uint2 T = gt[t];
-        const int a = tri_v(T, 0), b = tri_v(T, 1), c = tri_v(T, 2);
+        const TriU T = tri_get(V, t);
+        const int a = T.v[0], b = T.v[1], c = T.v[2];
         if (cyclic) {
             if ((a == sx && b == sy && c == sz) || (b == sx && c == sy && a == sz) || (c == sx && a == sy && b == sz))
                 return t;
@@ -770,11 +992,10 @@ __global__ void k_check(Dev D, unsigned long long* bad) {
     unsigned long long cnt = 0;
     for (int s = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); s < D.n; s += warps) {
         const StarHdr h = D.hdr[s];
-        const int* gh = D.hh + (size_t)s * HSLOTS;
-        const uint2* gt = D.tri + (size_t)s * TSTRIDE;
+        const StarView V = star_view(D, s);
         for (int t = lane; t < h.ntri; t += 32) {
-            const uint2 T = gt[t];
-            const int v[3] = {gh[tri_v(T, 0)] & (int)HID, gh[tri_v(T, 1)] & (int)HID, gh[tri_v(T, 2)] & (int)HID};
+            const TriU T = tri_get(V, t);
+            const int v[3] = {V.hh[T.v[0]] & (int)HID, V.hh[T.v[1]] & (int)HID, V.hh[T.v[2]] & (int)HID};
             for (int i = 0; i < 3; ++i)
                 if (find_tri(D, v[i], v[(i + 1) % 3], s, v[(i + 2) % 3], true) < 0) ++cnt;
         }
@@ -791,25 +1012,21 @@ __global__ void k_check(Dev D, unsigned long long* bad) {
 __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_tet_count(Dev D, int* cnt) {
     __shared__ int shh[WARPS_PER_BLOCK][HSLOTS];
     const int lane = threadIdx.x & 31;
-    int* hh = shh[threadIdx.x >> 5];
     const PredSink sink = sink_of(D);
     const int warps = gridDim.x * WARPS_PER_BLOCK;
     for (int s = blockIdx.x * WARPS_PER_BLOCK + (threadIdx.x >> 5); s < D.n; s += warps) {
         __syncwarp();  // the previous star's shared-memory reads are done
         const StarHdr h = D.hdr[s];
-        const int* gh = D.hh + (size_t)s * HSLOTS;
-        for (int k = lane; k < HSLOTS; k += 32) hh[k] = gh[k] & (int)HID;
-        __syncwarp();
-        uint2* gt = D.tri + (size_t)s * TSTRIDE;
+        const StarView V = star_view(D, s);
+        const int* ids = stage_ids(V, shh[threadIdx.x >> 5], lane);
         const double3 ps = gpt(D, s);
         int c = 0;
         for (int t = lane; t < h.ntri; t += 32) {
-            const uint2 T = gt[t];
-            const int a = hh[tri_v(T, 0)], b = hh[tri_v(T, 1)], cc = hh[tri_v(T, 2)];
+            const TriU T = tri_get(V, t);
+            const int a = ids[T.v[0]] & (int)HID, b = ids[T.v[1]] & (int)HID, cc = ids[T.v[2]] & (int)HID;
             bool keep = false;
             if (s < a && s < b && s < cc) keep = orient3d(gpt(D, a), gpt(D, b), gpt(D, cc), ps, sink) < 0;
-            const uint32_t nx = keep ? (T.x | TRI_KEPT) : (T.x & ~TRI_KEPT);
-            if (nx != T.x) gt[t].x = nx;
+            tri_set_kept(V, t, keep);
             c += keep;
         }
         for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
@@ -822,53 +1039,51 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_tet_count(Dev D, int* 
 __device__ int owned_tet_id(const Dev& D, const int* base, int star, int x, int y, int z) {
     const int ti = find_tri(D, star, x, y, z, false);
     if (ti < 0) return -1;
-    const uint2* gt = D.tri + (size_t)star * TSTRIDE;
-    if (!(gt[ti].x & TRI_KEPT)) return -1;
+    const StarView V = star_view(D, star);
+    if (!tri_kept(V, ti)) return -1;
     int r = 0;
-    for (int t = 0; t < ti; ++t) r += (int)(gt[t].x >> 31);
+    for (int t = 0; t < ti; ++t) r += tri_kept(V, t);
     return base[star] + r;
 }
 
 __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_tet_write(Dev D, const int* base, g4d_tet* tets,
                                                                     const int* sorted_to_input) {
     __shared__ int shh[WARPS_PER_BLOCK][HSLOTS];
-    __shared__ uint8_t srank[WARPS_PER_BLOCK][TSTRIDE];
+    __shared__ uint16_t srank[WARPS_PER_BLOCK][LTSTRIDE];
     const int lane = threadIdx.x & 31;
-    int* hh = shh[threadIdx.x >> 5];
-    uint8_t* rank = srank[threadIdx.x >> 5];
+    uint16_t* rank = srank[threadIdx.x >> 5];
     const int warps = gridDim.x * WARPS_PER_BLOCK;
     for (int s = blockIdx.x * WARPS_PER_BLOCK + (threadIdx.x >> 5); s < D.n; s += warps) {
         __syncwarp();  // the previous star's shared-memory reads are done
         const StarHdr h = D.hdr[s];
-        const int* gh = D.hh + (size_t)s * HSLOTS;
-        for (int k = lane; k < HSLOTS; k += 32) hh[k] = gh[k] & (int)HID;
-        const uint2* gt = D.tri + (size_t)s * TSTRIDE;
+        const StarView V = star_view(D, s);
+        const int* ids = stage_ids(V, shh[threadIdx.x >> 5], lane);
         int pre = 0;
         for (int b0 = 0; b0 < h.ntri; b0 += 32) {
             const int t = b0 + lane;
-            const bool kept = t < h.ntri && (gt[t].x & TRI_KEPT);
+            const bool kept = t < h.ntri && tri_kept(V, t);
             const unsigned m = __ballot_sync(0xffffffffu, kept);
-            if (t < h.ntri) rank[t] = (uint8_t)(pre + __popc(m & ((1u << lane) - 1u)));
+            if (t < h.ntri) rank[t] = (uint16_t)(pre + __popc(m & ((1u << lane) - 1u)));
             pre += __popc(m);
         }
         __syncwarp();
         for (int t = lane; t < h.ntri; t += 32) {
-            const uint2 T = gt[t];
-            if (!(T.x & TRI_KEPT)) continue;
-            const int sl[3] = {tri_v(T, 0), tri_v(T, 1), tri_v(T, 2)};
-            const int v[3] = {hh[sl[0]], hh[sl[1]], hh[sl[2]]};
+            const TriU T = tri_get(V, t);
+            if (!T.kept) continue;
+            const int* sl = T.v;
+            const int v[3] = {ids[sl[0]] & (int)HID, ids[sl[1]] & (int)HID, ids[sl[2]] & (int)HID};
             g4d_tet out;
             // neighbours across the faces that contain s: adjacent link triangles
             for (int i = 0; i < 3; ++i) {
-                const int oi = tri_o(T, i);
-                const uint2 N = gt[oi];
+                const int oi = T.o[i];
+                const TriU N = tri_get(V, oi);
                 const int e1 = sl[(i + 1) % 3], e2 = sl[(i + 2) % 3];
-                int xs = tri_v(N, 0);
+                int xs = N.v[0];
                 for (int k = 0; k < 3; ++k)
-                    if (tri_v(N, k) != e1 && tri_v(N, k) != e2) xs = tri_v(N, k);
-                const int x = hh[xs];
+                    if (N.v[k] != e1 && N.v[k] != e2) xs = N.v[k];
+                const int x = ids[xs] & (int)HID;
                 if (x > s)
-                    out.opp[i] = (N.x & TRI_KEPT) ? base[s] + rank[oi] : -1;
+                    out.opp[i] = N.kept ? base[s] + rank[oi] : -1;
                 else
                     out.opp[i] = owned_tet_id(D, base, x, s, v[(i + 1) % 3], v[(i + 2) % 3]);
             }
@@ -878,16 +1093,15 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_tet_write(Dev D, const
                 const int a = v[0], b = v[1], c = v[2];
                 const int ta = find_tri(D, a, b, s, c, false);
                 if (ta >= 0) {
-                    const int* ah = D.hh + (size_t)a * HSLOTS;
-                    const uint2* at = D.tri + (size_t)a * TSTRIDE;
-                    const uint2 A = at[ta];
+                    const StarView Va = star_view(D, a);
+                    const TriU A = tri_get(Va, ta);
                     int pos = 0;
                     for (int k = 0; k < 3; ++k)
-                        if ((ah[tri_v(A, k)] & (int)HID) == s) pos = k;
-                    const uint2 N = at[tri_o(A, pos)];
+                        if ((Va.hh[A.v[k]] & (int)HID) == s) pos = k;
+                    const TriU N = tri_get(Va, A.o[pos]);
                     int y = -1;
                     for (int k = 0; k < 3; ++k) {
-                        const int id = ah[tri_v(N, k)] & (int)HID;
+                        const int id = Va.hh[N.v[k]] & (int)HID;
                         if (id != b && id != c) y = id;
                     }
                     if (y >= 0) {
@@ -966,24 +1180,44 @@ void launch_eval_pred(const Launch& L, int kind, const double* pts, const int* i
 
 // --------------------------------------------------------------------------
 
-static int star_blocks(int items) {
-    int b = (items + WARPS_PER_BLOCK - 1) / WARPS_PER_BLOCK;
-    const int cap = 148 * 8;
+static int star_blocks(int items, int warps_per_block = WARPS_PER_BLOCK, int per_sm = 8) {
+    int b = (items + warps_per_block - 1) / warps_per_block;
+    const int cap = 148 * per_sm;
     if (b > cap) b = cap;
     return b < 1 ? 1 : b;
 }
 
-static size_t ws_bytes() { return sizeof(WS) * WARPS_PER_BLOCK; }
-
 void launch_star_build(const Launch& L, const Dev& D) {
-    cudaFuncSetAttribute(k_star_build, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ws_bytes());
-    k_star_build<<<star_blocks(D.n), 32 * WARPS_PER_BLOCK, ws_bytes(), L.stream>>>(D);
+    const size_t sm = sizeof(WS<SmallStar>) * WARPS_PER_BLOCK;
+    cudaFuncSetAttribute(k_star_build, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_star_build<<<star_blocks(D.n), 32 * WARPS_PER_BLOCK, sm, L.stream>>>(D);
     ++*L.launches;
 }
 
 void launch_star_insert(const Launch& L, const Dev& D, int count) {
-    cudaFuncSetAttribute(k_star_insert, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ws_bytes());
-    k_star_insert<<<star_blocks(count), 32 * WARPS_PER_BLOCK, ws_bytes(), L.stream>>>(D, count);
+    const size_t sm = sizeof(WS<SmallStar>) * SmallStar::WARPS;
+    cudaFuncSetAttribute(k_star_insert<SmallStar>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_star_insert<SmallStar><<<star_blocks(count), 32 * SmallStar::WARPS, sm, L.stream>>>(D, D.wlIns, count);
+    ++*L.launches;
+}
+
+void launch_star_insert_large(const Launch& L, const Dev& D, const int* list, int count) {
+    const size_t sm = sizeof(WS<LargeStar>) * LargeStar::WARPS;
+    cudaFuncSetAttribute(k_star_insert<LargeStar>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_star_insert<LargeStar><<<star_blocks(count, LargeStar::WARPS, 2), 32 * LargeStar::WARPS, sm, L.stream>>>(
+        D, list, count);
+    ++*L.launches;
+}
+
+void launch_promote(const Launch& L, const Dev& D, int count) {
+    k_promote<<<star_blocks(count), 32 * WARPS_PER_BLOCK, 0, L.stream>>>(D, count);
+    ++*L.launches;
+}
+
+void launch_requeue(const Launch& L, const Dev& D, int count) {
+    int b = (count + 127) / 128;
+    if (b > 148 * 8) b = 148 * 8;
+    k_requeue<<<b < 1 ? 1 : b, 128, 0, L.stream>>>(D, count);
     ++*L.launches;
 }
 

@@ -82,6 +82,8 @@ typedef struct {
     int grid_size;               /* grid actually used */
     int tets;
     long long gpu_launches;      /* kernels launched by this call */
+    int large_stars;             /* stars that outgrew the small storage class */
+    int spare;
 } g4d_stats;
 
 typedef struct g4d_ctx g4d_ctx;

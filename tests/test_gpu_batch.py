@@ -1,0 +1,79 @@
+"""Batched triangulation (g4d_triangulate_batch) against one call per cloud and
+against the oracle. Needs a B200.
+
+Every cloud of a batch must come back bit-exact: the same canonical
+tetrahedra and adjacency, in cloud-local input indices, as the same cloud
+triangulated alone at the same grid width.
+"""
+import numpy as np
+import pytest
+
+from gstar4d_b200 import workloads
+
+pytestmark = pytest.mark.gpu
+
+
+def auto_grid(n):
+    g = 32
+    while g ** 3 < 134 * n and g < 1024:
+        g *= 2
+    return g
+
+
+def _batch(count, seed, hi):
+    sizes = workloads.batch_sizes(count, seed=seed, hi=hi)
+    clouds = [workloads.batch_cloud(int(n), kind=i % 3, seed=seed * 1000 + i) for i, n in enumerate(sizes)]
+    offs = np.zeros(len(clouds) + 1, np.int64)
+    offs[1:] = np.cumsum([len(c) for c in clouds])
+    return clouds, np.concatenate(clouds), offs
+
+
+def _canon(oracle, tets):
+    import gstar4d_b200
+    return oracle.canonical(gstar4d_b200.tets_as_array(tets))
+
+
+def test_batch_matches_single_cloud_calls(oracle):
+    import gstar4d_b200
+    clouds, pts, offs = _batch(48, seed=3, hi=6000)
+    with gstar4d_b200.Triangulator() as t:
+        tets, toffs, stats = t.triangulate_batch(pts, offs)
+        assert len(toffs) == len(clouds) + 1 and toffs[-1] == len(tets)
+        for c, cloud in enumerate(clouds):
+            single, _, _ = t.triangulate(cloud)
+            got = _canon(oracle, tets[toffs[c]:toffs[c + 1]])
+            exp = _canon(oracle, single)
+            assert np.array_equal(got[0], exp[0]), "cloud %d: tetrahedra differ" % c
+            assert np.array_equal(got[1], exp[1]), "cloud %d: adjacency differs" % c
+    # a few clouds against the oracle itself
+    for c in (0, 7, 20):
+        ref, _, _ = oracle.triangulate(clouds[c], auto_grid(len(clouds[c])))
+        got = _canon(oracle, tets[toffs[c]:toffs[c + 1]])
+        exp = oracle.canonical(ref)
+        assert np.array_equal(got[0], exp[0]) and np.array_equal(got[1], exp[1]), c
+
+
+def test_batch_fixed_grid_and_repeat_calls(oracle):
+    """All clouds on one grid width (one stack), and a second call on the same
+    context reusing its buffers."""
+    import gstar4d_b200
+    clouds, pts, offs = _batch(12, seed=4, hi=3000)
+    with gstar4d_b200.Triangulator(grid_size=64) as t:
+        a, ao, _ = t.triangulate_batch(pts, offs)
+        b, bo, _ = t.triangulate_batch(pts, offs)
+    assert np.array_equal(ao, bo)
+    for c in range(len(clouds)):
+        ref, _, _ = oracle.triangulate(clouds[c], 64)
+        for tets, toffs in ((a, ao), (b, bo)):
+            got = _canon(oracle, tets[toffs[c]:toffs[c + 1]])
+            exp = oracle.canonical(ref)
+            assert np.array_equal(got[0], exp[0]) and np.array_equal(got[1], exp[1]), c
+
+
+def test_batch_rejects_tiny_cloud():
+    import gstar4d_b200
+    pts = np.random.default_rng(1).random((20, 3))
+    with gstar4d_b200.Triangulator() as t:
+        with pytest.raises(gstar4d_b200.G4DError) as e:
+            t.triangulate_batch(pts, np.array([0, 3, 20], np.int64))
+    assert e.value.status == 1

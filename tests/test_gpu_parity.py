@@ -69,6 +69,23 @@ def test_parity_uniform_100k_full_size(oracle):
     assert np.array_equal(g[0], r[0]) and np.array_equal(g[1], r[1])
 
 
+def test_parity_degenerate500k_with_large_stars(oracle):
+    """The 500,000-point degenerate configuration (sphere + lattice + uniform,
+    grid 512^3): stars next to the dense sphere sheet outgrow the small storage
+    class and finish in the large class; the result stays bit-exact, exact
+    predicates and Simulation of Simplicity included."""
+    import gstar4d_b200
+    pts, G = workloads.config_cloud("degenerate500k")
+    with gstar4d_b200.Triangulator(grid_size=G, do_check=1) as t:
+        tets, _, stats = t.triangulate(pts)
+    assert stats["large_stars"] > 0
+    assert stats["exact_predicates"] > 0
+    ref, _, _ = oracle.triangulate(pts, G)
+    g, r = _canon(oracle, tets), oracle.canonical(ref)
+    assert np.array_equal(g[0], r[0]), "tetrahedra differ"
+    assert np.array_equal(g[1], r[1]), "adjacency differs"
+
+
 def test_morton_index_space_and_gdel_entry_points(oracle):
     """gdelInit/gdelCompute/getTetraFromGpu shape: points already in grid units,
     overwritten with the Morton order; output in Morton indices."""
