@@ -11,6 +11,7 @@ the batched entry point. Failures raise G4DError carrying the C status code;
 the CUDA library is required (there is no CPU fallback).
 """
 import ctypes
+import weakref
 import os
 
 import numpy as np
@@ -59,7 +60,8 @@ _lib = None
 
 EXPORTS = ["g4d_default_config", "g4d_create", "g4d_destroy", "g4d_last_error", "g4d_status_string",
            "g4d_triangulate", "g4d_triangulate_to", "g4d_triangulate_device", "g4d_gdel_init",
-           "g4d_gdel_compute", "g4d_get_tetra", "g4d_gdel_deinit", "g4d_triangulate_batch", "g4d_stream",
+           "g4d_gdel_compute", "g4d_get_tetra", "g4d_gdel_deinit", "g4d_triangulate_batch",
+           "g4d_triangulate_batch_device", "g4d_stream",
            "g4d_eval_predicates", "g4d_voronoi", "g4d_voronoi_noalloc", "g4d_free"]
 
 
@@ -88,6 +90,8 @@ def load():
     L.g4d_gdel_deinit.argtypes = [vp]
     L.g4d_triangulate_batch.argtypes = [vp, vp, vp, ip, ctypes.POINTER(vp), ctypes.POINTER(vp),
                                         ctypes.POINTER(Stats)]
+    L.g4d_triangulate_batch_device.argtypes = [vp, vp, vp, ip, ctypes.POINTER(vp), ctypes.POINTER(vp),
+                                               ctypes.POINTER(Stats)]
     L.g4d_eval_predicates.argtypes = [vp, ip, vp, vp, ip, vp]
     L.g4d_voronoi.argtypes = [vp, vp, ip, ip, vp]
     L.g4d_voronoi_noalloc.argtypes = [vp, ip, ip, vp, vp]
@@ -244,13 +248,35 @@ class Triangulator:
                                              ctypes.byref(op), ctypes.byref(stats))
         self._check(st)
         toffs = np.frombuffer((ctypes.c_int64 * (nclouds + 1)).from_address(op.value), np.int64).copy()
-        total = int(toffs[-1])
-        tets = np.frombuffer((ctypes.c_char * max(total * TET_DTYPE.itemsize, 1)).from_address(tp.value),
-                             TET_DTYPE)[:total].copy()
-        self._lib.g4d_free(tp)
         self._lib.g4d_free(op)
+        total = int(toffs[-1])
+        # the library's buffer becomes the array's memory (freed with the array)
+        tets = _adopt(self._lib, tp.value, total * TET_DTYPE.itemsize, TET_DTYPE, total)
         self.last_stats = stats.as_dict()
         return tets, toffs, self.last_stats
+
+    def triangulate_batch_device(self, d_points, cloud_offsets):
+        """Batch on device-resident points (d_points: device address of n*3
+        doubles). Returns (device address of the tetrahedra, their count, tet
+        offsets per cloud, stats); the device buffer belongs to the context."""
+        offs = np.ascontiguousarray(cloud_offsets, dtype=np.int64)
+        tp, op = ctypes.c_void_p(), ctypes.c_void_p()
+        stats = Stats()
+        nclouds = len(offs) - 1
+        st = self._lib.g4d_triangulate_batch_device(self._h, ctypes.c_void_p(int(d_points)), _ptr(offs), nclouds,
+                                                    ctypes.byref(tp), ctypes.byref(op), ctypes.byref(stats))
+        self._check(st)
+        toffs = np.frombuffer((ctypes.c_int64 * (nclouds + 1)).from_address(op.value), np.int64).copy()
+        self.last_stats = stats.as_dict()
+        return tp.value, int(toffs[-1]), toffs, self.last_stats
+
+
+def _adopt(lib, ptr, nbytes, dtype, count):
+    """numpy view of a library-allocated buffer that frees it (g4d_free) when
+    the last view is gone."""
+    buf = (ctypes.c_char * max(nbytes, 1)).from_address(ptr)
+    weakref.finalize(buf, lib.g4d_free, ctypes.c_void_p(ptr))
+    return np.frombuffer(buf, dtype)[:count]
 
 
 def tets_as_array(tets):

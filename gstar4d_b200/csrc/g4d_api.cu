@@ -15,6 +15,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <map>
 #include <vector>
 
 #include "g4d_internal.cuh"
@@ -50,7 +51,7 @@ enum BufId {
     B_XYZ, B_GRIDSRC, B_MM, B_KEYS, B_VALS, B_VOXIN, B_MKEY, B_ORDER, B_P, B_VOX, B_CKEY0, B_CID0, B_CKEY,
     B_CID, B_COLS, B_COLE, B_GA, B_GB, B_BUCKET, B_BCOUNT, B_HH, B_TRI, B_HDR, B_INBOX, B_ICOUNT, B_WLINS,
     B_WLEMIT, B_WLEMIT2, B_DROWN, B_DROWN2, B_CTR, B_CNT, B_BASE, B_TETS, B_CUB, B_BAD, B_LIDX, B_LHH, B_LTRI,
-    B_WLINSL, B_WLPROM, B_SKEY0, B_SKEY, B_GIDX, B_LOCAL, B_BCKEY0, B_BCKEY, B_SLOTS, B_MMB, B_TC, B_TETS2, B_OVF, B_OVF2, B_NUM
+    B_WLINSL, B_WLPROM, B_SKEY0, B_SKEY, B_GIDX, B_LOCAL, B_BCKEY0, B_BCKEY, B_SLOTS, B_MMB, B_TC, B_TETS2, B_OVF, B_OVF2, B_KMASK, B_BOUT, B_OCC, B_NUM
 };
 
 }  // namespace
@@ -74,6 +75,9 @@ struct g4d_ctx {
     std::vector<double> gdel_points;
     bool gdel_ready = false;
     cudaEvent_t ev[8];
+    std::map<int, int> tuned;  // autotuner: (size bucket, distribution class) -> grid width
+    int next_grid = 0;         // tuned width for the next single-cloud call (0: none)
+    std::vector<int64_t> batch_offsets;  // tet offsets of the last device batch
 };
 
 namespace {
@@ -135,6 +139,7 @@ Dev make_dev(g4d_ctx* ctx) {
     D.wlInsL = ctx->b[B_WLINSL].as<int>();
     D.wlPromote = ctx->b[B_WLPROM].as<int>();
     D.anyLarge = 0;
+    D.keptMask = ctx->b[B_KMASK].as<uint32_t>();
     D.ovf = ctx->b[B_OVF].as<int2>();
     D.ovfNext = ctx->b[B_OVF2].as<int2>();
     D.ovfCap = (int)(std::min(ctx->b[B_OVF].cap, ctx->b[B_OVF2].cap) / sizeof(int2));
@@ -191,7 +196,8 @@ g4d_status check_err(g4d_ctx* ctx, unsigned e) {
     }
     if (e & ERR_CAPACITY)
         return fail(ctx, G4D_ERR_CAPACITY, "a star exceeded %d points / %d triangles (large class)", LHMAX, LTMAX);
-    if (e & ERR_DROWNCAP) return fail(ctx, G4D_ERR_CAPACITY, "drowned or overflow request list capacity exceeded");
+    if (e & ERR_DROWNCAP) return fail(ctx, G4D_ERR_CAPACITY, "drowned list capacity exceeded");
+    if (e & ERR_OVFCAP) return fail(ctx, G4D_ERR_CAPACITY, "overflow request list capacity exceeded");
     return fail(ctx, G4D_ERR_INTERNAL, "star topology error (flags 0x%x)", e);
 }
 
@@ -276,8 +282,27 @@ g4d_status alloc_stars(g4d_ctx* ctx, int n) {
     CK(ctx->b[B_BAD].ensure(64));
     CK(ctx->b[B_LIDX].ensure(sizeof(int) * n));
     CK(ctx->b[B_WLPROM].ensure(sizeof(int) * n));
-    CK(ctx->b[B_OVF].ensure(sizeof(int2) * 4 * (size_t)n));
-    CK(ctx->b[B_OVF2].ensure(sizeof(int2) * 4 * (size_t)n));
+    CK(ctx->b[B_OVF].ensure(sizeof(int2) * (8 * (size_t)n + 1024)));
+    CK(ctx->b[B_OVF2].ensure(sizeof(int2) * (8 * (size_t)n + 1024)));
+    CK(ctx->b[B_KMASK].ensure(sizeof(uint32_t) * (TSTRIDE / 32) * (size_t)n));
+    return G4D_OK;
+}
+
+// Grow both overflow request lists to hold `need` entries, keeping the
+// current list's first `keep` entries.
+g4d_status grow_ovf(g4d_ctx* ctx, Dev& D, int keep, size_t need) {
+    void *a = nullptr, *b = nullptr;
+    CK(cudaMalloc(&a, sizeof(int2) * need));
+    CK(cudaMalloc(&b, sizeof(int2) * need));
+    if (keep > 0) CK(cudaMemcpyAsync(a, D.ovf, sizeof(int2) * keep, cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->b[B_OVF].release();
+    ctx->b[B_OVF2].release();
+    ctx->b[B_OVF].p = a; ctx->b[B_OVF].cap = sizeof(int2) * need;
+    ctx->b[B_OVF2].p = b; ctx->b[B_OVF2].cap = sizeof(int2) * need;
+    D.ovf = static_cast<int2*>(a);
+    D.ovfNext = static_cast<int2*>(b);
+    D.ovfCap = (int)std::min<size_t>(need, 0x7fffffff);
     return G4D_OK;
 }
 
@@ -308,11 +333,22 @@ g4d_status run_splay(g4d_ctx* ctx, Dev& D) {
     const int max_loops = 4000;
     for (;; ++loops) {
         if (loops >= max_loops) return fail(ctx, G4D_ERR_TIMEOUT, "splaying did not converge in %d loops", max_loops);
-        if (ovfCount) launch_requeue(L, D, std::min(ovfCount, D.ovfCap));
-        if (drownCount) launch_proof(L, D, drownCount);
-        if (emitCount) launch_emit(L, D, emitCount);
-        CK(cudaMemcpyAsync(&h, dctr, sizeof(Counters), cudaMemcpyDeviceToHost, ctx->stream));
-        CK(cudaStreamSynchronize(ctx->stream));
+        // emission phase; it only adds (deduplicated) inbox requests, so when the
+        // overflow list ran out it is grown and the phase repeated
+        for (int attempt = 0;; ++attempt) {
+            if (ovfCount) launch_requeue(L, D, ovfCount);
+            if (drownCount) launch_proof(L, D, drownCount);
+            if (emitCount) launch_emit(L, D, emitCount);
+            CK(cudaMemcpyAsync(&h, dctr, sizeof(Counters), cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+            if (!(h.err & ERR_OVFCAP) || attempt >= 3) break;
+            st = grow_ovf(ctx, D, ovfCount, 2 * (size_t)h.ovf_next + (size_t)D.n);
+            if (st) return st;
+            CK(cudaMemsetAsync(&dctr->ovf_next, 0, sizeof(int), ctx->stream));
+            const unsigned clear = ~(unsigned)ERR_OVFCAP;
+            h.err &= clear;
+            CK(cudaMemcpyAsync(&dctr->err, &h.err, sizeof(unsigned), cudaMemcpyHostToDevice, ctx->stream));
+        }
         st = check_err(ctx, h.err);
         if (st) return st;
         if (h.ins_count == 0 && h.ins_count_large == 0) break;
@@ -444,7 +480,8 @@ g4d_status check_n(g4d_ctx* ctx, int n) {
 }
 
 g4d_status pick_grid(g4d_ctx* ctx, int n) {
-    int G = ctx->cfg.grid_size > 0 ? ctx->cfg.grid_size : auto_grid(n);
+    int G = ctx->cfg.grid_size > 0 ? ctx->cfg.grid_size : (ctx->next_grid > 0 ? ctx->next_grid : auto_grid(n));
+    ctx->next_grid = 0;
     if (G < 32 || G > 1024 || (G & (G - 1)))
         return fail(ctx, G4D_ERR_ARG, "grid size must be a power of two in [32, 1024] (got %d)", G);
     ctx->G = G;
@@ -485,20 +522,31 @@ int bits_for(unsigned long long v) {
     return b;
 }
 
-struct BatchOut {
-    g4d_tet* tets = nullptr;
-    size_t count = 0, cap = 0;
-};
+// Device-side batch output: tetrahedra of all waves back to back (cloud order
+// within each wave, waves in cloud order), grown by copying when needed.
+g4d_status reserve_out(g4d_ctx* ctx, size_t used, size_t need) {
+    Buf& o = ctx->b[B_BOUT];
+    if (need * sizeof(g4d_tet) <= o.cap && o.p) return G4D_OK;
+    const size_t want = std::max(need, used + used / 2) * sizeof(g4d_tet) + 256;
+    void* np = nullptr;
+    CK(cudaMalloc(&np, want));
+    if (used && o.p) CK(cudaMemcpyAsync(np, o.p, used * sizeof(g4d_tet), cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    o.release();
+    o.p = np;
+    o.cap = want;
+    return G4D_OK;
+}
 
-// clouds[c0..c1) of the batch, grid widths in Gc; appends the wave's
-// tetrahedra (cloud order, cloud-local ids) to out and fills tet counts.
-g4d_status run_wave(g4d_ctx* ctx, const double* d_xyz, const int64_t* offs, int c0, int c1, const int* Gc,
-                    BatchOut& out, int64_t* tet_counts) {
+// One wave over the clouds cl[0..ns) (grid widths Gc[cloud]): their tetrahedra,
+// in list order with cloud-local ids, are written to the batch output from
+// element `at` on; tet_counts[cloud] receives each cloud's count.
+g4d_status run_wave(g4d_ctx* ctx, const double* d_xyz, const int64_t* offs, const int* cl, int ns, const int* Gc,
+                    size_t at, int64_t* tet_counts, size_t* wave_tets) {
     Launch L{ctx->stream, &ctx->launches};
-    const int ns = c1 - c0;
     // slots: clouds ordered by grid width (stable)
-    std::vector<int> slot_cloud(ns);
-    for (int k = 0; k < ns; ++k) slot_cloud[k] = c0 + k;
+    std::vector<int> slot_cloud(cl, cl + ns);
+    std::vector<int> list_pos(ns);
     std::stable_sort(slot_cloud.begin(), slot_cloud.end(), [&](int a, int b) { return Gc[a] < Gc[b]; });
     std::vector<long long> slotIn(ns), slotCol(ns);
     std::vector<int> slotW(ns + 1), slotG(ns);
@@ -613,34 +661,211 @@ g4d_status run_wave(g4d_ctx* ctx, const double* d_xyz, const int64_t* offs, int 
     if (st) return st;
     st = run_extract(ctx, D, nullptr);
     if (st) return st;
-    // per-cloud counts and output offsets in cloud order
+    // per-cloud counts and output offsets in list order
     const int ntet = ctx->ntet;
     launch_b_slot_tets(L, ctx->b[B_BASE].as<int>(), d_slotW, ns, d_tc);
     std::vector<int> tc(ns);
     CK(cudaMemcpyAsync(tc.data(), d_tc, sizeof(int) * ns, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    std::vector<long long> cnt_cloud(ns), dst(ns);
-    for (int k = 0; k < ns; ++k) cnt_cloud[slot_cloud[k] - c0] = tc[k];
-    std::vector<long long> off_cloud(ns + 1, 0);
-    for (int c = 0; c < ns; ++c) off_cloud[c + 1] = off_cloud[c] + cnt_cloud[c];
-    for (int k = 0; k < ns; ++k) dst[k] = off_cloud[slot_cloud[k] - c0];
-    for (int c = 0; c < ns; ++c) tet_counts[c0 + c] = cnt_cloud[c];
-    CK(cudaMemcpyAsync(d_dst, dst.data(), i64b, cudaMemcpyHostToDevice, ctx->stream));
-    CK(ctx->b[B_TETS2].ensure(sizeof(g4d_tet) * (size_t)std::max(ntet, 1)));
-    launch_b_localize(L, ctx->b[B_TETS].as<g4d_tet>(), ntet, skey, ctx->b[B_LOCAL].as<int>(),
-                      ctx->b[B_BASE].as<int>(), d_slotW, d_dst, ctx->b[B_TETS2].as<g4d_tet>());
-    // host output
-    if (out.count + (size_t)ntet > out.cap) {
-        size_t ncap = std::max(out.cap * 2, out.count + (size_t)ntet);
-        g4d_tet* p = (g4d_tet*)realloc(out.tets, sizeof(g4d_tet) * std::max<size_t>(ncap, 1));
-        if (!p) return fail(ctx, G4D_ERR_NOMEM, "host allocation of %zu tetrahedra failed", ncap);
-        out.tets = p;
-        out.cap = ncap;
+    std::vector<int> pos_of(ns);  // slot -> position of its cloud in the list
+    {
+        std::vector<std::pair<int, int>> lp(ns);
+        for (int i = 0; i < ns; ++i) lp[i] = {cl[i], i};
+        std::sort(lp.begin(), lp.end());
+        for (int k = 0; k < ns; ++k) {
+            const auto it = std::lower_bound(lp.begin(), lp.end(), std::make_pair(slot_cloud[k], -1));
+            pos_of[k] = it->second;
+        }
     }
-    CK(cudaMemcpyAsync(out.tets + out.count, ctx->b[B_TETS2].p, sizeof(g4d_tet) * (size_t)ntet,
-                       cudaMemcpyDeviceToHost, ctx->stream));
+    std::vector<long long> cnt_pos(ns), off_pos(ns + 1, 0), dst(ns);
+    for (int k = 0; k < ns; ++k) cnt_pos[pos_of[k]] = tc[k];
+    for (int i = 0; i < ns; ++i) off_pos[i + 1] = off_pos[i] + cnt_pos[i];
+    for (int k = 0; k < ns; ++k) dst[k] = (long long)at + off_pos[pos_of[k]];
+    for (int i = 0; i < ns; ++i) tet_counts[cl[i]] = cnt_pos[i];
+    CK(cudaMemcpyAsync(d_dst, dst.data(), i64b, cudaMemcpyHostToDevice, ctx->stream));
+    st = reserve_out(ctx, at, at + (size_t)ntet);
+    if (st) return st;
+    launch_b_localize(L, ctx->b[B_TETS].as<g4d_tet>(), ntet, skey, ctx->b[B_LOCAL].as<int>(),
+                      ctx->b[B_BASE].as<int>(), d_slotW, d_dst, ctx->b[B_BOUT].as<g4d_tet>());
+    cudaEventRecord(ctx->ev[6], ctx->stream);
+    CK(cudaEventSynchronize(ctx->ev[6]));  // stage times are read right after
+    *wave_tets = (size_t)ntet;
+    return G4D_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Autotuner: grid width per cloud. The reference fixes G by flag; its default
+// density is about 134 voxels per point. Sparse grids make the digital Voronoi
+// passes expensive (their cost follows the voxel count), dense ones leave more
+// points sharing voxels and more work for splaying. For every (size bucket,
+// distribution class) the tuner times waves of up to kTuneClouds sample clouds
+// at the density rule's width and at one half and one quarter of it, and keeps
+// the fastest; later clouds of that key reuse the choice (per context).
+// ---------------------------------------------------------------------------
+
+constexpr int kTuneClouds = 16;
+
+// Distribution class: occupancy of an 8^3 histogram of a strided sample of up
+// to 4096 points against what a uniform sample of that size fills.
+// 0 = spread out (uniform-like), 1 = intermediate, 2 = concentrated.
+int class_of(int filled, int64_t n) {
+    const double m = (double)std::min<int64_t>(n, 4096);
+    const double expect = 512.0 * (1.0 - std::exp(-m / 512.0));
+    const double r = filled / expect;
+    return r > 0.6 ? 0 : (r > 0.25 ? 1 : 2);
+}
+
+// host restatement of k_b_occupancy (same sample, same arithmetic order)
+int occupancy(const double* xyz, int64_t n) {
+    const int64_t m = std::min<int64_t>(n, 4096);
+    const int64_t step = std::max<int64_t>(1, n / m);
+    double lo = xyz[0], hi = xyz[0];
+    for (int64_t i = 0; i < m; ++i)
+        for (int c = 0; c < 3; ++c) {
+            const double v = xyz[3 * (i * step) + c];
+            lo = std::min(lo, v);
+            hi = std::max(hi, v);
+        }
+    const double span = hi > lo ? hi - lo : 1.0;
+    uint32_t bits[16] = {0};
+    for (int64_t i = 0; i < m; ++i) {
+        int q[3];
+        for (int c = 0; c < 3; ++c) {
+            volatile double d = xyz[3 * (i * step) + c] - lo;  // no contraction: the device rounds each step
+            volatile double e = 8.0 * d;
+            q[c] = std::min(7, (int)(e / span));
+        }
+        const int cell = (q[2] * 8 + q[1]) * 8 + q[0];
+        bits[cell >> 5] |= 1u << (cell & 31);
+    }
+    int f = 0;
+    for (int w = 0; w < 16; ++w) f += __builtin_popcount(bits[w]);
+    return f;
+}
+
+int tune_key(int64_t n, int dclass) { return bits_for((unsigned long long)n) * 4 + dclass; }
+
+// grid widths for every cloud; tunes the keys not yet in the context's table
+g4d_status pick_batch_grids(g4d_ctx* ctx, const double* d_xyz, const int64_t* offs, int nclouds,
+                            std::vector<int>& Gc) {
+    Gc.assign(std::max(nclouds, 1), 0);
+    if (ctx->cfg.grid_size > 0 || ctx->cfg.grid_size == 0) {
+        for (int c = 0; c < nclouds; ++c) {
+            const int64_t n = offs[c + 1] - offs[c];
+            Gc[c] = ctx->cfg.grid_size > 0 ? ctx->cfg.grid_size : auto_grid((int)n);
+        }
+        return G4D_OK;
+    }
+    // distribution classes from the device copy of the points
+    CK(ctx->b[B_OCC].ensure(sizeof(long long) * (nclouds + 1) + sizeof(int) * nclouds + 64));
+    long long* d_offs = ctx->b[B_OCC].as<long long>();
+    int* d_occ = reinterpret_cast<int*>(d_offs + nclouds + 1);
+    CK(cudaMemcpyAsync(d_offs, offs, sizeof(long long) * (nclouds + 1), cudaMemcpyHostToDevice, ctx->stream));
+    Launch L{ctx->stream, &ctx->launches};
+    launch_b_occupancy(L, d_xyz, d_offs, nclouds, d_occ);
+    std::vector<int> occ(nclouds);
+    CK(cudaMemcpyAsync(occ.data(), d_occ, sizeof(int) * nclouds, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    out.count += ntet;
+    std::vector<int> key(nclouds);
+    std::map<int, std::vector<int>> pending;
+    for (int c = 0; c < nclouds; ++c) {
+        const int64_t n = offs[c + 1] - offs[c];
+        key[c] = tune_key(n, class_of(occ[c], n));
+        if (!ctx->tuned.count(key[c])) {
+            auto& v = pending[key[c]];
+            if ((int)v.size() < kTuneClouds) v.push_back(c);
+        }
+    }
+    for (auto& kv : pending) {
+        const std::vector<int>& sample = kv.second;
+        long long pts = 0;
+        for (int c : sample) pts += offs[c + 1] - offs[c];
+        const int g0 = auto_grid((int)std::max<long long>(5, pts / (long long)sample.size()));
+        int best = g0;
+        float best_ms = 1e30f;
+        std::vector<int> Gs(nclouds, 0);
+        std::vector<int64_t> cnt(nclouds, 0);
+        const double avg = (double)pts / (double)sample.size();
+        for (int pass = 0; pass < 4; ++pass) {
+            const int g = pass == 0 ? g0 : std::max(32, g0 >> (pass - 1));  // first pass warms up
+            if (pass > 1 && g == std::max(32, g0 >> (pass - 2))) break;
+            if (pass > 1 && (double)g * g * g < 8.0 * avg) break;  // under 8 voxels per point
+            for (int c : sample) Gs[c] = g;
+            size_t wt = 0;
+            g4d_status st = run_wave(ctx, d_xyz, offs, sample.data(), (int)sample.size(), Gs.data(), 0, cnt.data(), &wt);
+            if (st && pass <= 1) return st;
+            if (st) break;  // a denser candidate that fails is not taken
+            const float ms = ms_between(ctx->ev[0], ctx->ev[6]);
+            if (ctx->cfg.log_verbose)
+                fprintf(stderr, "autotune: %zu clouds, %.0f points avg, class %d: G=%d %.3f ms%s\n", sample.size(),
+                        avg, kv.first & 3, g, ms, pass == 0 ? " (warm-up)" : "");
+            if (pass > 0 && ms < best_ms) { best_ms = ms; best = g; }
+        }
+        ctx->tuned[kv.first] = best;
+    }
+    for (int c = 0; c < nclouds; ++c) Gc[c] = ctx->tuned[key[c]];
+    return G4D_OK;
+}
+
+// All waves of a batch whose points are on the device; the tetrahedra end in
+// B_BOUT (cloud order) and counts[c] per cloud.
+g4d_status run_batch(g4d_ctx* ctx, const double* d_xyz, const int64_t* offs, int nclouds,
+                     std::vector<int64_t>& counts, size_t* total, g4d_stats* acc) {
+    for (int c = 0; c < nclouds; ++c) {
+        const int64_t n = offs[c + 1] - offs[c];
+        if (n < 5 || n >= (1 << 30))
+            return fail(ctx, G4D_ERR_ARG, "cloud %d has %lld points (need 5 or more)", c, (long long)n);
+    }
+    if (nclouds && offs[0] != 0) return fail(ctx, G4D_ERR_ARG, "cloud_offsets[0] must be 0");
+    std::vector<int> Gc;
+    g4d_status st = pick_batch_grids(ctx, d_xyz, offs, nclouds, Gc);
+    if (st) return st;
+    for (int c = 0; c < nclouds; ++c)
+        if (Gc[c] < 32 || Gc[c] > 1024 || (Gc[c] & (Gc[c] - 1)))
+            return fail(ctx, G4D_ERR_ARG, "grid size must be a power of two in [32, 1024] (got %d)", Gc[c]);
+    ctx->launches = 0;
+    counts.assign(nclouds, 0);
+    // reserve output for about 7 tetrahedra per point (grown if exceeded)
+    const int64_t npts = nclouds ? offs[nclouds] : 0;
+    st = reserve_out(ctx, 0, (size_t)(7.2 * (double)npts) + 1024);
+    if (st) return st;
+    size_t at = 0;
+    int large = 0;
+    std::vector<int> list;
+    for (int c0 = 0; c0 < nclouds;) {
+        int c1 = c0;
+        long long pts = 0, vox = 0;
+        while (c1 < nclouds) {
+            const long long n = offs[c1 + 1] - offs[c1];
+            const long long v = (long long)Gc[c1] * Gc[c1] * Gc[c1];
+            if (c1 > c0 && (pts + n > kWavePoints || vox + v > kWaveVoxels)) break;
+            pts += n;
+            vox += v;
+            ++c1;
+        }
+        list.resize(c1 - c0);
+        for (int c = c0; c < c1; ++c) list[c - c0] = c;
+        size_t wt = 0;
+        st = run_wave(ctx, d_xyz, offs, list.data(), c1 - c0, Gc.data(), at, counts.data(), &wt);
+        if (st) return st;
+        at += wt;
+        acc->t_init_ms += ms_between(ctx->ev[0], ctx->ev[1]);
+        acc->t_pba_ms += ms_between(ctx->ev[1], ctx->ev[2]);
+        acc->t_star_ms += ms_between(ctx->ev[2], ctx->ev[3]);
+        acc->t_splay_ms += ms_between(ctx->ev[3], ctx->ev[4]);
+        acc->t_out_ms += ms_between(ctx->ev[4], ctx->ev[6]);
+        acc->splay_insertions += ctx->stats.splay_insertions;
+        acc->proofs += ctx->stats.proofs;
+        acc->exact_predicates += ctx->stats.exact_predicates;
+        acc->loops = std::max(acc->loops, ctx->stats.loops);
+        large += ctx->large_used;
+        c0 = c1;
+    }
+    *total = at;
+    acc->tets = (int)std::min<size_t>(at, 0x7fffffff);
+    acc->gpu_launches = ctx->launches;
+    acc->large_stars = large;
+    acc->grid_size = nclouds ? *std::max_element(Gc.begin(), Gc.begin() + nclouds) : 0;
     return G4D_OK;
 }
 
@@ -729,6 +954,21 @@ g4d_status g4d_triangulate_device(g4d_ctx* ctx, const double* d_xyz, int n, cons
     if (st) return st;
     if (!d_xyz || !d_tets || !ntet) return fail(ctx, G4D_ERR_ARG, "null argument");
     cudaSetDevice(ctx->device);
+    if (ctx->cfg.grid_size < 0 && !ctx->tuned.empty()) {
+        // autotuned mode: the distribution class from the device copy of the points
+        const long long offs[2] = {0, n};
+        CK(ctx->b[B_OCC].ensure(sizeof(long long) * 2 + sizeof(int) + 64));
+        long long* d_offs = ctx->b[B_OCC].as<long long>();
+        int* d_occ = reinterpret_cast<int*>(d_offs + 2);
+        CK(cudaMemcpyAsync(d_offs, offs, sizeof(offs), cudaMemcpyHostToDevice, ctx->stream));
+        Launch L{ctx->stream, &ctx->launches};
+        launch_b_occupancy(L, d_xyz, d_offs, 1, d_occ);
+        int occ = 0;
+        CK(cudaMemcpyAsync(&occ, d_occ, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        const auto it = ctx->tuned.find(tune_key(n, class_of(occ, n)));
+        if (it != ctx->tuned.end()) ctx->next_grid = it->second;
+    }
     st = run_all_device(ctx, d_xyz, nullptr, n, ctx->cfg.index_space == 0);
     if (st) return st;
     *d_tets = ctx->b[B_TETS].as<g4d_tet>();
@@ -743,6 +983,11 @@ g4d_status g4d_triangulate_to(g4d_ctx* ctx, const double* xyz, int n, g4d_tet* o
     if (st) return st;
     if (!xyz || !ntet) return fail(ctx, G4D_ERR_ARG, "null argument");
     cudaSetDevice(ctx->device);
+    if (ctx->cfg.grid_size < 0) {
+        // autotuned mode: reuse the width tuned for this size and distribution
+        const auto it = ctx->tuned.find(tune_key(n, class_of(occupancy(xyz, n), n)));
+        if (it != ctx->tuned.end()) ctx->next_grid = it->second;
+    }
     CK(ctx->b[B_XYZ].ensure(sizeof(double) * 3 * (size_t)n));
     CK(cudaMemcpyAsync(ctx->b[B_XYZ].p, xyz, sizeof(double) * 3 * (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
     st = run_all_device(ctx, ctx->b[B_XYZ].as<double>(), nullptr, n, ctx->cfg.index_space == 0);
@@ -857,60 +1102,50 @@ g4d_status g4d_triangulate_batch(g4d_ctx* ctx, const double* xyz, const int64_t*
     *tet_offsets = nullptr;
     cudaSetDevice(ctx->device);
     const auto t0 = std::chrono::steady_clock::now();
-    std::vector<int> Gc(std::max(nclouds, 1));
-    for (int c = 0; c < nclouds; ++c) {
-        const int64_t n = cloud_offsets[c + 1] - cloud_offsets[c];
-        if (n < 5 || n >= (1 << 30)) return fail(ctx, G4D_ERR_ARG, "cloud %d has %lld points (need 5 or more)", c, (long long)n);
-        const int G = ctx->cfg.grid_size > 0 ? ctx->cfg.grid_size : auto_grid((int)n);
-        if (G < 32 || G > 1024 || (G & (G - 1)))
-            return fail(ctx, G4D_ERR_ARG, "grid size must be a power of two in [32, 1024] (got %d)", G);
-        Gc[c] = G;
-    }
-    const int64_t total = nclouds ? cloud_offsets[nclouds] - cloud_offsets[0] : 0;
-    if (nclouds && cloud_offsets[0] != 0) return fail(ctx, G4D_ERR_ARG, "cloud_offsets[0] must be 0");
-    ctx->launches = 0;
-    memset(&ctx->stats, 0, sizeof(ctx->stats));
+    const int64_t total = nclouds ? cloud_offsets[nclouds] : 0;
     CK(ctx->b[B_XYZ].ensure(sizeof(double) * 3 * (size_t)std::max<int64_t>(total, 1)));
     CK(cudaMemcpyAsync(ctx->b[B_XYZ].p, xyz, sizeof(double) * 3 * (size_t)total, cudaMemcpyHostToDevice, ctx->stream));
-    std::vector<int64_t> counts(nclouds, 0);
-    BatchOut out;
+    std::vector<int64_t> counts;
+    size_t ntet = 0;
     g4d_stats acc{};
-    int large = 0;
-    for (int c0 = 0; c0 < nclouds;) {
-        int c1 = c0;
-        long long pts = 0, vox = 0;
-        while (c1 < nclouds) {
-            const long long n = cloud_offsets[c1 + 1] - cloud_offsets[c1];
-            const long long v = (long long)Gc[c1] * Gc[c1] * Gc[c1];
-            if (c1 > c0 && (pts + n > kWavePoints || vox + v > kWaveVoxels)) break;
-            pts += n;
-            vox += v;
-            ++c1;
-        }
-        g4d_status st = run_wave(ctx, ctx->b[B_XYZ].as<double>(), cloud_offsets, c0, c1, Gc.data(), out,
-                                 counts.data());
-        if (st) { free(out.tets); return st; }
-        acc.t_pba_ms += ms_between(ctx->ev[1], ctx->ev[2]);
-        acc.t_star_ms += ms_between(ctx->ev[2], ctx->ev[3]);
-        acc.t_splay_ms += ms_between(ctx->ev[3], ctx->ev[4]);
-        acc.t_out_ms += ms_between(ctx->ev[4], ctx->ev[5]);
-        acc.splay_insertions += ctx->stats.splay_insertions;
-        acc.proofs += ctx->stats.proofs;
-        acc.exact_predicates += ctx->stats.exact_predicates;
-        acc.loops = std::max(acc.loops, ctx->stats.loops);
-        large += ctx->large_used;
-        c0 = c1;
-    }
+    g4d_status st = run_batch(ctx, ctx->b[B_XYZ].as<double>(), cloud_offsets, nclouds, counts, &ntet, &acc);
+    if (st) return st;
+    g4d_tet* out = (g4d_tet*)malloc(sizeof(g4d_tet) * std::max<size_t>(ntet, 1));
     int64_t* offs = (int64_t*)malloc(sizeof(int64_t) * (nclouds + 1));
-    if (!offs) { free(out.tets); return fail(ctx, G4D_ERR_NOMEM, "host allocation failed"); }
+    if (!out || !offs) {
+        free(out);
+        free(offs);
+        return fail(ctx, G4D_ERR_NOMEM, "host allocation of %zu tetrahedra failed", ntet);
+    }
+    CK(cudaMemcpyAsync(out, ctx->b[B_BOUT].p, sizeof(g4d_tet) * ntet, cudaMemcpyDeviceToHost, ctx->stream));
     offs[0] = 0;
     for (int c = 0; c < nclouds; ++c) offs[c + 1] = offs[c] + counts[c];
-    if (!out.tets) out.tets = (g4d_tet*)malloc(sizeof(g4d_tet));
-    *tets = out.tets;
+    CK(cudaStreamSynchronize(ctx->stream));
+    *tets = out;
     *tet_offsets = offs;
-    acc.tets = (int)std::min<size_t>(out.count, 0x7fffffff);
-    acc.gpu_launches = ctx->launches;
-    acc.large_stars = large;
+    acc.t_total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    ctx->stats = acc;
+    if (stats) *stats = acc;
+    return G4D_OK;
+}
+
+g4d_status g4d_triangulate_batch_device(g4d_ctx* ctx, const double* d_xyz, const int64_t* cloud_offsets,
+                                        int nclouds, const g4d_tet** d_tets, const int64_t** tet_offsets,
+                                        g4d_stats* stats) {
+    if (!ctx) return G4D_ERR_ARG;
+    if (!d_xyz || !cloud_offsets || nclouds < 0 || !d_tets || !tet_offsets)
+        return fail(ctx, G4D_ERR_ARG, "null argument");
+    cudaSetDevice(ctx->device);
+    const auto t0 = std::chrono::steady_clock::now();
+    std::vector<int64_t> counts;
+    size_t ntet = 0;
+    g4d_stats acc{};
+    g4d_status st = run_batch(ctx, d_xyz, cloud_offsets, nclouds, counts, &ntet, &acc);
+    if (st) return st;
+    ctx->batch_offsets.assign(nclouds + 1, 0);
+    for (int c = 0; c < nclouds; ++c) ctx->batch_offsets[c + 1] = ctx->batch_offsets[c] + counts[c];
+    *d_tets = ctx->b[B_BOUT].as<g4d_tet>();
+    *tet_offsets = ctx->batch_offsets.data();
     acc.t_total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     ctx->stats = acc;
     if (stats) *stats = acc;

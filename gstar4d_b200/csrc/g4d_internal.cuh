@@ -4,9 +4,11 @@
 //   P        double4[n]     points in Morton order (x,y,z,0): one 32-byte sector each
 //   vox      uint32[n]      voxel of each point, packed x | y<<10 | z<<20
 //   grid A/B uint32[G^3]    digital Voronoi sites, packed voxel coords, x fastest
-//   hh       int32[n*256]   per-star history hash: every point ever inserted in the
+//   hh       int32[n*512]   per-star history hash: every point ever inserted in the
 //                           star (bit 31 = currently in the link), open addressing
-//   tri      uint2[n*256]   per-star link triangles, 8 bytes each (see TriPack)
+//   tri      uint2[n*224]   per-star link triangles, 8 bytes each (packing below)
+//   lhh/ltri                the same for the few stars promoted to the large class
+//                           (2048 hash slots, 1024 triangles of 16 bytes)
 //   hdr      StarHdr[n]     triangle count, history count, pass number, flags
 //   bucket   int32[n*64]    initial candidate worksets (Voronoi pairs + missing)
 //   inbox    int32[n*64]    insertion requests for the next splaying round
@@ -38,8 +40,8 @@ constexpr uint32_t MARKER = 0xffffffffu;  // voxel without a site
 // sampled sphere) moves to the large class between kernels.
 constexpr int HSLOTS = 512;               // small: history hash slots per star
 constexpr int HMAX = 255;                 // small: max history entries (hash load <= 1/2)
-constexpr int TMAX = 252;                 // small: max link triangles (2 * HMAX - 4)
-constexpr int TSTRIDE = 256;              // small: triangle slots per star in HBM
+constexpr int TMAX = 220;                 // small: max link triangles (a link of 112 points)
+constexpr int TSTRIDE = 224;              // small: triangle slots per star in HBM
 constexpr int LHSLOTS = 2048;             // large: history hash slots
 constexpr int LHMAX = 1023;               // large: max history entries
 constexpr int LTMAX = 1020;               // large: max link triangles
@@ -58,6 +60,7 @@ enum : unsigned {
     ERR_TOPOLOGY = 4u,   // a hole that is not a disk, or every triangle beneath
     ERR_PROOF = 8u,      // no containment proof found
     ERR_DROWNCAP = 16u,  // drowned list full
+    ERR_OVFCAP = 32u,    // overflow request list full (the host grows it and repeats the emission phase)
 };
 
 // star header flags
@@ -150,6 +153,7 @@ struct Dev {
     int* wlInsL;           // large stars with inbox requests
     int* wlPromote;        // small stars to move to the large class
     int anyLarge;          // some star is in the large class (else lidx is not read)
+    uint32_t* keptMask;    // small stars: kept-triangle bits (TSTRIDE / 32 words each)
     // requests (star, point) that found the star's inbox full: re-sent next round
     int2* ovf;
     int2* ovfNext;
@@ -185,6 +189,7 @@ void launch_b_gather(const Launch& L, const double* xyz, const long long* gidx, 
 void launch_b_colkeys(const Launch& L, const uint32_t* vox, const unsigned long long* skey, const int* slotG,
                       const long long* slotCol, int n, unsigned long long* ckey, int* cid);
 void launch_colranges_u64(const Launch& L, const unsigned long long* ckey, int n, int* colStart, int* colEnd);
+void launch_b_occupancy(const Launch& L, const double* xyz, const long long* offs, int nclouds, int* occ);
 void launch_b_slot_tets(const Launch& L, const int* base, const int* slotW, int nslots, int* tc);
 void launch_b_localize(const Launch& L, const g4d_tet* in, int ntet, const unsigned long long* skey,
                        const int* local, const int* base, const int* slotW, const long long* dst, g4d_tet* out);

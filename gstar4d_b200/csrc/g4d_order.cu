@@ -273,6 +273,62 @@ __global__ void k_b_localize(const g4d_tet* __restrict__ in, int ntet, const uns
     }
 }
 
+// Distribution class input: occupancy of an 8^3 histogram of a strided sample
+// of up to 4096 points of each cloud (one block per cloud). The host function
+// occupancy() in g4d_api.cu does the same arithmetic in the same order.
+__global__ void k_b_occupancy(const double* __restrict__ xyz, const long long* __restrict__ offs, int* __restrict__ occ) {
+    __shared__ unsigned long long slo[8], shi[8];
+    __shared__ unsigned bits[16];
+    const int c = blockIdx.x;
+    const long long n = offs[c + 1] - offs[c];
+    const long long m = n < 4096 ? n : 4096;
+    const long long step = n / m > 1 ? n / m : 1;
+    const double* p = xyz + 3 * offs[c];
+    unsigned long long lo = ~0ull, hi = 0ull;
+    for (long long k = threadIdx.x; k < 3 * m; k += blockDim.x) {
+        const unsigned long long v = dkey(p[3 * ((k / 3) * step) + k % 3]);
+        lo = v < lo ? v : lo;
+        hi = v > hi ? v : hi;
+    }
+    for (int o = 16; o; o >>= 1) {
+        const unsigned long long a = __shfl_xor_sync(0xffffffffu, lo, o);
+        const unsigned long long b = __shfl_xor_sync(0xffffffffu, hi, o);
+        lo = a < lo ? a : lo;
+        hi = b > hi ? b : hi;
+    }
+    if (threadIdx.x < 16) bits[threadIdx.x] = 0;
+    if ((threadIdx.x & 31) == 0) { slo[threadIdx.x >> 5] = lo; shi[threadIdx.x >> 5] = hi; }
+    __syncthreads();
+    lo = slo[0];
+    hi = shi[0];
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+        lo = slo[w] < lo ? slo[w] : lo;
+        hi = shi[w] > hi ? shi[w] : hi;
+    }
+    const double dlo = dkey_inv(lo), dhi = dkey_inv(hi);
+    const double span = dhi > dlo ? __dsub_rn(dhi, dlo) : 1.0;
+    for (long long i = threadIdx.x; i < m; i += blockDim.x) {
+        int q[3];
+        for (int k = 0; k < 3; ++k) {
+            const int b = (int)__ddiv_rn(__dmul_rn(8.0, __dsub_rn(p[3 * (i * step) + k], dlo)), span);
+            q[k] = b < 7 ? b : 7;
+        }
+        const int cell = (q[2] * 8 + q[1]) * 8 + q[0];
+        atomicOr(&bits[cell >> 5], 1u << (cell & 31));
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int f = 0;
+        for (int w = 0; w < 16; ++w) f += __popc(bits[w]);
+        occ[c] = f;
+    }
+}
+
+void launch_b_occupancy(const Launch& L, const double* xyz, const long long* offs, int nclouds, int* occ) {
+    k_b_occupancy<<<nclouds, 256, 0, L.stream>>>(xyz, offs, occ);
+    ++*L.launches;
+}
+
 void launch_b_order(const Launch& L, const double* xyz, int nslots, const long long* slotIn, const int* slotW,
                     const int* slotG, unsigned long long* mm, unsigned long long* keys, int* vals, uint32_t* vox_in,
                     long long* gidx, unsigned* err) {

@@ -32,7 +32,7 @@ constexpr int WARPS_PER_BLOCK = 4;
 
 struct SmallStar {
     static constexpr int LOG2_HS = 9, HS = HSLOTS, HM = HMAX, TM = TMAX, TS = TSTRIDE;
-    static constexpr int WARPS = WARPS_PER_BLOCK, MINB = 3;
+    static constexpr int WARPS = WARPS_PER_BLOCK, MINB = 4;
     static constexpr bool LARGE = false;
     using Idx = uint8_t;   // triangle index and coordinate-cache index
     using Rec = uint32_t;  // hole boundary edge: u | w<<9 | o<<18 | oj<<26
@@ -94,7 +94,8 @@ struct LargeStar {
     __device__ static Tri* tris(const Dev& D, int s) { return D.ltri + (size_t)D.lidx[s] * TS; }
 };
 
-// Per-warp shared-memory image of one star (16 KB small, 80 KB large).
+// Per-warp shared-memory image of one star (14 KB small, so that 16 warps fit
+// on an SM; 76 KB large).
 template <class C>
 struct WS {
     using Idx = typename C::Idx;
@@ -105,16 +106,21 @@ struct WS {
     Idx to[3][C::TS];              // neighbour across the edge opposite each vertex
     uint8_t tj[3][C::TS];          // position of the shared edge inside that neighbour
     uint8_t tf[C::TS];             // bit 7 alive, bits 0..3 creation pass
-    Idx efrom[C::HS], eto[C::HS];
-    typename C::Rec erec[C::TS];   // hole boundary edges
+    Idx efrom[C::HM + 1], eto[C::HM + 1];  // by coordinate-cache index of the edge's vertex
+    union {
+        typename C::Rec erec[C::TS];  // hole boundary edges (insertion)
+        float okey[C::HM + 1];        // squared distances (initial sort, before any insertion)
+    };
     Idx blist[C::TS];              // beneath triangles in index order / compaction map
     Idx fstack[C::TS];             // free triangle slots
     uint16_t order[C::HM + 1];     // insertion order (slots)
-    float okey[C::HM + 1];
     uint32_t bmask[C::TS / 32];
     uint32_t wasLink[C::HS / 32], insMask[C::HS / 32];
     int nedge, nfree, ntri, nins, nhist, ncoord;
 };
+
+// 4 blocks of 4 warps per SM: 16 images plus the per-block reservation in 228 KB
+static_assert(4 * (4 * sizeof(WS<SmallStar>) + 1024) <= 228 * 1024, "small star image too large");
 
 // Read-only view of any star, whichever class holds it (cross-star lookups).
 struct StarView {
@@ -282,7 +288,7 @@ __device__ __forceinline__ void push_inbox(const Dev& D, int t, int v, bool* ove
         *overflow = true;
         const int q = atomicAdd(&D.ctr->ovf_next, 1);
         if (q < D.ovfCap) D.ovfNext[q] = make_int2(t, v);
-        else atomicOr(&D.ctr->err, ERR_DROWNCAP);
+        else atomicOr(&D.ctr->err, ERR_OVFCAP);
     }
 }
 
@@ -400,21 +406,21 @@ __device__ int warp_insert(WS<C>& S, int lane, int s, double3 ps, int sp, int ge
             const int rr = r - nb;
             slot = rr < nfree ? S.fstack[nfree - 1 - rr] : ntri + (rr - nfree);
         }
-        S.efrom[u] = (Idx)slot;
-        S.eto[w] = (Idx)slot;
+        S.efrom[S.cix[u]] = (Idx)slot;
+        S.eto[S.cix[w]] = (Idx)slot;
     }
     __syncwarp();
     // new triangle (u, w, p) replaces the beneath triangle across the edge u->w
     for (int r = lane; r < B; r += 32) {
         const typename C::Rec e = S.erec[r];
         const int u = C::rec_u(e), w = C::rec_w(e), o = C::rec_o(e), oj = C::rec_oj(e);
-        const int slot = S.efrom[u];
+        const int slot = S.efrom[S.cix[u]];
         S.tv[0][slot] = (uint16_t)u;
         S.tv[1][slot] = (uint16_t)w;
         S.tv[2][slot] = (uint16_t)sp;
-        S.to[0][slot] = S.efrom[w];  // edge (w, p): the next boundary edge's triangle
+        S.to[0][slot] = S.efrom[S.cix[w]];  // edge (w, p): the next boundary edge's triangle
         S.tj[0][slot] = 1;
-        S.to[1][slot] = S.eto[u];    // edge (p, u): the previous boundary edge's triangle
+        S.to[1][slot] = S.eto[S.cix[u]];    // edge (p, u): the previous boundary edge's triangle
         S.tj[1][slot] = 0;
         S.to[2][slot] = (Idx)o;      // edge (u, w): the triangle outside the hole
         S.tj[2][slot] = (uint8_t)oj;
@@ -604,9 +610,9 @@ __device__ void warp_store(WS<C>& S, const Dev& D, int lane, int s, int pass, bo
 // BUCKET_CAP + MIN_WORKSET points, so always the small class)
 // --------------------------------------------------------------------------
 
-// 3 blocks per SM: shared memory (about 65 KB per block) allows no more, and
-// this register budget (168) costs only a few hundred bytes of spills.
-__global__ void __launch_bounds__(32 * WARPS_PER_BLOCK, 3) k_star_build(Dev D) {
+// 4 blocks per SM: shared memory (about 57 KB per block) allows no more, and
+// this register budget (128) costs only a few hundred bytes of spills.
+__global__ void __launch_bounds__(32 * WARPS_PER_BLOCK, 4) k_star_build(Dev D) {
     G4D_DYN_SMEM(smem_raw);
     using C = SmallStar;
     const int lane = threadIdx.x & 31;
@@ -962,18 +968,29 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_proof(Dev D, int count
 // appear as the cyclic triangle (b,s,c) in star a
 // --------------------------------------------------------------------------
 
-// index of the triangle of `star` with vertex ids {x,y,z} (cyclic x,y,z when
-// `cyclic`), or -1
-__device__ int find_tri(const Dev& D, int star, int x, int y, int z, bool cyclic) {
-    if (!valid_id(D, star)) return -1;
-    const StarView V = star_view(D, star);
-    uint32_t e;
-    const int sx = view_lookup(V, x, &e), sy = view_lookup(V, y, &e), sz = view_lookup(V, z, &e);
+// slot of id v in a class-C history hash, -1 if absent
+template <class C>
+__device__ __forceinline__ int hash_slot(const int* h, int v) {
+    uint32_t s = hslot0<C::LOG2_HS>(v);
+    for (int k = 0; k < C::HS; ++k) {
+        const uint32_t e = (uint32_t)h[s];
+        if ((e & HID) == (uint32_t)v) return (int)s;
+        if ((e & HID) == HEMPTY) return -1;
+        s = (s + 1) & (C::HS - 1);
+    }
+    return -1;
+}
+
+// index of the triangle with vertex ids {x,y,z} (cyclic x,y,z when `cyclic`)
+// in a class-C star, or -1
+template <class C>
+__device__ __forceinline__ int find_tri_t(const int* h, const typename C::Tri* gt, int ntri, int x, int y, int z,
+                                          bool cyclic) {
+    const int sx = hash_slot<C>(h, x), sy = hash_slot<C>(h, y), sz = hash_slot<C>(h, z);
     if (sx < 0 || sy < 0 || sz < 0) return -1;
-    const StarHdr hd = D.hdr[star];
-    for (int t = 0; t < hd.ntri; ++t) {
-        const TriU T = tri_get(V, t);
-        const int a = T.v[0], b = T.v[1], c = T.v[2];
+    for (int t = 0; t < ntri; ++t) {
+        const typename C::Tri T = gt[t];
+        const int a = C::tv(T, 0), b = C::tv(T, 1), c = C::tv(T, 2);
         if (cyclic) {
             if ((a == sx && b == sy && c == sz) || (b == sx && c == sy && a == sz) || (c == sx && a == sy && b == sz))
                 return t;
@@ -984,6 +1001,14 @@ __device__ int find_tri(const Dev& D, int star, int x, int y, int z, bool cyclic
         }
     }
     return -1;
+}
+
+__device__ int find_tri(const Dev& D, int star, int x, int y, int z, bool cyclic) {
+    if (!valid_id(D, star)) return -1;
+    const StarView V = star_view(D, star);
+    const int ntri = D.hdr[star].ntri;
+    return V.large ? find_tri_t<LargeStar>(V.hh, static_cast<const uint4*>(V.tri), ntri, x, y, z, cyclic)
+                   : find_tri_t<SmallStar>(V.hh, static_cast<const uint2*>(V.tri), ntri, x, y, z, cyclic);
 }
 
 __global__ void k_check(Dev D, unsigned long long* bad) {
@@ -1006,7 +1031,10 @@ __global__ void k_check(Dev D, unsigned long long* bad) {
 
 // --------------------------------------------------------------------------
 // extraction (GDelHost.cu:1520-1607): owner triangle (star < its 3 vertices) on
-// the lower hull, orient3d(v0,v1,v2,star) < 0, is a Delaunay tetrahedron
+// the lower hull, orient3d(v0,v1,v2,star) < 0, is a Delaunay tetrahedron. The
+// tetrahedra of star s are numbered base[s] + (rank of the triangle among the
+// star's kept triangles); small stars keep a bit mask of their kept triangles
+// so that any star's rank is a few popcounts.
 // --------------------------------------------------------------------------
 
 __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_tet_count(Dev D, int* cnt) {
@@ -1021,12 +1049,17 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_tet_count(Dev D, int* 
         const int* ids = stage_ids(V, shh[threadIdx.x >> 5], lane);
         const double3 ps = gpt(D, s);
         int c = 0;
-        for (int t = lane; t < h.ntri; t += 32) {
-            const TriU T = tri_get(V, t);
-            const int a = ids[T.v[0]] & (int)HID, b = ids[T.v[1]] & (int)HID, cc = ids[T.v[2]] & (int)HID;
+        for (int b0 = 0; b0 < h.ntri; b0 += 32) {
+            const int t = b0 + lane;
             bool keep = false;
-            if (s < a && s < b && s < cc) keep = orient3d(gpt(D, a), gpt(D, b), gpt(D, cc), ps, sink) < 0;
-            tri_set_kept(V, t, keep);
+            if (t < h.ntri) {
+                const TriU T = tri_get(V, t);
+                const int a = ids[T.v[0]] & (int)HID, b = ids[T.v[1]] & (int)HID, cc = ids[T.v[2]] & (int)HID;
+                if (s < a && s < b && s < cc) keep = orient3d(gpt(D, a), gpt(D, b), gpt(D, cc), ps, sink) < 0;
+                tri_set_kept(V, t, keep);
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, keep);
+            if (!V.large && lane == 0) D.keptMask[(size_t)s * (TSTRIDE / 32) + (b0 >> 5)] = m;
             c += keep;
         }
         for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
@@ -1037,13 +1070,108 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_tet_count(Dev D, int* 
 // tet id of the kept tetrahedron owned by `star` (its smallest vertex) whose
 // other vertices are {x,y,z}, or -1
 __device__ int owned_tet_id(const Dev& D, const int* base, int star, int x, int y, int z) {
-    const int ti = find_tri(D, star, x, y, z, false);
-    if (ti < 0) return -1;
+    if (!valid_id(D, star)) return -1;
     const StarView V = star_view(D, star);
-    if (!tri_kept(V, ti)) return -1;
+    const int ntri = D.hdr[star].ntri;
+    if (!V.large) {
+        const int ti = find_tri_t<SmallStar>(V.hh, static_cast<const uint2*>(V.tri), ntri, x, y, z, false);
+        if (ti < 0) return -1;
+        const uint32_t* m = D.keptMask + (size_t)star * (TSTRIDE / 32);
+        const uint32_t mw = m[ti >> 5];
+        if (!((mw >> (ti & 31)) & 1u)) return -1;
+        int r = __popc(mw & ((1u << (ti & 31)) - 1u));
+        for (int w = 0; w < (ti >> 5); ++w) r += __popc(m[w]);
+        return base[star] + r;
+    }
+    const int ti = find_tri_t<LargeStar>(V.hh, static_cast<const uint4*>(V.tri), ntri, x, y, z, false);
+    if (ti < 0 || !tri_kept(V, ti)) return -1;
     int r = 0;
     for (int t = 0; t < ti; ++t) r += tri_kept(V, t);
     return base[star] + r;
+}
+
+// the vertex y beyond edge (b,c) from s in star a: the triangle (b, s, c) of
+// star a and its neighbour across (b, c) = (b, c, y); -1 if absent
+template <class C>
+__device__ __forceinline__ int across_t(const int* h, const typename C::Tri* gt, int ntri, int s, int b, int c) {
+    const int ta = find_tri_t<C>(h, gt, ntri, b, s, c, false);
+    if (ta < 0) return -1;
+    const typename C::Tri A = gt[ta];
+    int pos = 0;
+    for (int k = 0; k < 3; ++k)
+        if ((h[C::tv(A, k)] & (int)HID) == s) pos = k;
+    const typename C::Tri N = gt[C::to(A, pos)];
+    int y = -1;
+    for (int k = 0; k < 3; ++k) {
+        const int id = h[C::tv(N, k)] & (int)HID;
+        if (id != b && id != c) y = id;
+    }
+    return y;
+}
+
+// neighbour of tetrahedron (a, b, c, s) across the face (a, b, c), or -1
+__device__ int face_neighbor(const Dev& D, const int* base, int s, int a, int b, int c) {
+    if (!valid_id(D, a)) return -1;
+    const StarView Va = star_view(D, a);
+    const int ntri = D.hdr[a].ntri;
+    const int y = Va.large ? across_t<LargeStar>(Va.hh, static_cast<const uint4*>(Va.tri), ntri, s, b, c)
+                           : across_t<SmallStar>(Va.hh, static_cast<const uint2*>(Va.tri), ntri, s, b, c);
+    if (y < 0) return -1;
+    const int all4[4] = {a, b, c, y};
+    int m = a;
+    for (int k = 1; k < 4; ++k) m = all4[k] < m ? all4[k] : m;
+    int q[3], nq = 0;
+    for (int k = 0; k < 4; ++k)
+        if (all4[k] != m && nq < 3) q[nq++] = all4[k];
+    return nq == 3 ? owned_tet_id(D, base, m, q[0], q[1], q[2]) : -1;
+}
+
+// tetrahedra owned by star s (a warp)
+template <class C>
+__device__ __forceinline__ void write_star(const Dev& D, const int* base, g4d_tet* tets, const int* sorted_to_input,
+                                           int s, int ntri, const int* ids, const typename C::Tri* gt,
+                                           uint16_t* rank, int lane) {
+    int pre = 0;
+    for (int b0 = 0; b0 < ntri; b0 += 32) {
+        const int t = b0 + lane;
+        const bool kept = t < ntri && C::kept(gt[t]);
+        const unsigned m = __ballot_sync(0xffffffffu, kept);
+        if (t < ntri) rank[t] = (uint16_t)(pre + __popc(m & ((1u << lane) - 1u)));
+        pre += __popc(m);
+    }
+    __syncwarp();
+    for (int t = lane; t < ntri; t += 32) {
+        const typename C::Tri T = gt[t];
+        if (!C::kept(T)) continue;
+        const int sl[3] = {C::tv(T, 0), C::tv(T, 1), C::tv(T, 2)};
+        const int v[3] = {ids[sl[0]] & (int)HID, ids[sl[1]] & (int)HID, ids[sl[2]] & (int)HID};
+        g4d_tet out;
+        // neighbours across the faces that contain s: adjacent link triangles
+        for (int i = 0; i < 3; ++i) {
+            const int oi = C::to(T, i);
+            const typename C::Tri N = gt[oi];
+            const int e1 = sl[(i + 1) % 3], e2 = sl[(i + 2) % 3];
+            int xs = C::tv(N, 0);
+            for (int k = 0; k < 3; ++k)
+                if (C::tv(N, k) != e1 && C::tv(N, k) != e2) xs = C::tv(N, k);
+            const int x = ids[xs] & (int)HID;
+            if (x > s)
+                out.opp[i] = C::kept(N) ? base[s] + rank[oi] : -1;
+            else
+                out.opp[i] = owned_tet_id(D, base, x, s, v[(i + 1) % 3], v[(i + 2) % 3]);
+        }
+        // neighbour across the face (v0, v1, v2): through star v0
+        out.opp[3] = face_neighbor(D, base, s, v[0], v[1], v[2]);
+        if (sorted_to_input) {
+            out.v[0] = sorted_to_input[v[0]];
+            out.v[1] = sorted_to_input[v[1]];
+            out.v[2] = sorted_to_input[v[2]];
+            out.v[3] = sorted_to_input[s];
+        } else {
+            out.v[0] = v[0]; out.v[1] = v[1]; out.v[2] = v[2]; out.v[3] = s;
+        }
+        tets[base[s] + rank[t]] = out;
+    }
 }
 
 __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_tet_write(Dev D, const int* base, g4d_tet* tets,
@@ -1058,74 +1186,12 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_tet_write(Dev D, const
         const StarHdr h = D.hdr[s];
         const StarView V = star_view(D, s);
         const int* ids = stage_ids(V, shh[threadIdx.x >> 5], lane);
-        int pre = 0;
-        for (int b0 = 0; b0 < h.ntri; b0 += 32) {
-            const int t = b0 + lane;
-            const bool kept = t < h.ntri && tri_kept(V, t);
-            const unsigned m = __ballot_sync(0xffffffffu, kept);
-            if (t < h.ntri) rank[t] = (uint16_t)(pre + __popc(m & ((1u << lane) - 1u)));
-            pre += __popc(m);
-        }
-        __syncwarp();
-        for (int t = lane; t < h.ntri; t += 32) {
-            const TriU T = tri_get(V, t);
-            if (!T.kept) continue;
-            const int* sl = T.v;
-            const int v[3] = {ids[sl[0]] & (int)HID, ids[sl[1]] & (int)HID, ids[sl[2]] & (int)HID};
-            g4d_tet out;
-            // neighbours across the faces that contain s: adjacent link triangles
-            for (int i = 0; i < 3; ++i) {
-                const int oi = T.o[i];
-                const TriU N = tri_get(V, oi);
-                const int e1 = sl[(i + 1) % 3], e2 = sl[(i + 2) % 3];
-                int xs = N.v[0];
-                for (int k = 0; k < 3; ++k)
-                    if (N.v[k] != e1 && N.v[k] != e2) xs = N.v[k];
-                const int x = ids[xs] & (int)HID;
-                if (x > s)
-                    out.opp[i] = N.kept ? base[s] + rank[oi] : -1;
-                else
-                    out.opp[i] = owned_tet_id(D, base, x, s, v[(i + 1) % 3], v[(i + 2) % 3]);
-            }
-            // neighbour across the face (v0, v1, v2): through star v0
-            {
-                int res = -1;
-                const int a = v[0], b = v[1], c = v[2];
-                const int ta = find_tri(D, a, b, s, c, false);
-                if (ta >= 0) {
-                    const StarView Va = star_view(D, a);
-                    const TriU A = tri_get(Va, ta);
-                    int pos = 0;
-                    for (int k = 0; k < 3; ++k)
-                        if ((Va.hh[A.v[k]] & (int)HID) == s) pos = k;
-                    const TriU N = tri_get(Va, A.o[pos]);
-                    int y = -1;
-                    for (int k = 0; k < 3; ++k) {
-                        const int id = Va.hh[N.v[k]] & (int)HID;
-                        if (id != b && id != c) y = id;
-                    }
-                    if (y >= 0) {
-                        const int all4[4] = {a, b, c, y};
-                        int m = a;
-                        for (int k = 1; k < 4; ++k) m = all4[k] < m ? all4[k] : m;
-                        int q[3], nq = 0;
-                        for (int k = 0; k < 4; ++k)
-                            if (all4[k] != m && nq < 3) q[nq++] = all4[k];
-                        if (nq == 3) res = owned_tet_id(D, base, m, q[0], q[1], q[2]);
-                    }
-                }
-                out.opp[3] = res;
-            }
-            if (sorted_to_input) {
-                out.v[0] = sorted_to_input[v[0]];
-                out.v[1] = sorted_to_input[v[1]];
-                out.v[2] = sorted_to_input[v[2]];
-                out.v[3] = sorted_to_input[s];
-            } else {
-                out.v[0] = v[0]; out.v[1] = v[1]; out.v[2] = v[2]; out.v[3] = s;
-            }
-            tets[base[s] + rank[t]] = out;
-        }
+        if (!V.large)
+            write_star<SmallStar>(D, base, tets, sorted_to_input, s, h.ntri, ids, static_cast<const uint2*>(V.tri),
+                                  rank, lane);
+        else
+            write_star<LargeStar>(D, base, tets, sorted_to_input, s, h.ntri, ids, static_cast<const uint4*>(V.tri),
+                                  rank, lane);
     }
 }
 

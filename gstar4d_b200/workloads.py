@@ -66,6 +66,18 @@ def batch_sizes(count=4096, seed=1, lo=64, hi=50000):
     return np.floor(np.exp(rng.uniform(np.log(lo), np.log(hi), size=count))).astype(np.int64)
 
 
+def batch_clouds(count=4096, seed=1, hi=50000):
+    """The 4,096-cloud batch: sizes log-uniform in [64, hi], each cloud uniform,
+    Gaussian (sigma 0.1) or an 8-cluster mixture (sigma 0.02) by a seeded draw.
+    Returns (list of clouds, concatenated points, int64 offsets)."""
+    sizes = batch_sizes(count, seed=seed, hi=hi)
+    kinds = np.random.default_rng(seed + 7).integers(0, 3, size=count)
+    clouds = [batch_cloud(int(n), int(k), seed * 100003 + i) for i, (n, k) in enumerate(zip(sizes, kinds))]
+    offs = np.zeros(count + 1, np.int64)
+    offs[1:] = np.cumsum([len(c) for c in clouds])
+    return clouds, np.concatenate(clouds), offs
+
+
 def batch_cloud(n, kind, seed):
     rng = np.random.default_rng(seed)
     if kind == 0:

@@ -50,7 +50,10 @@ typedef enum {
 typedef struct {
     int seed;            /* -s   (CLI point generation) */
     int run_num;         /* -r */
-    int grid_size;       /* -g   PBA grid width G: power of two, 32..1024; 0 = autotune */
+    int grid_size;       /* -g   PBA grid width G: power of two, 32..1024; 0 = the reference's
+                            density (about 134 voxels per point); -1 = autotuned (batches time
+                            sample waves per size bucket and distribution; single clouds reuse
+                            a width tuned on the same context) */
     int point_num;       /* -n */
     int dist;            /* -d   0 uniform, 1 gaussian, 2 ball, 3 sphere, 4 grid */
     int facet_max;       /* -f   kept for flag compatibility (no effect: no per-loop bound) */
@@ -131,13 +134,27 @@ G4D_API g4d_status g4d_gdel_compute(g4d_ctx* ctx, double* t_pba, double* t_star,
 G4D_API g4d_status g4d_get_tetra(g4d_ctx* ctx, const g4d_tet** tets, int* ntet);
 G4D_API g4d_status g4d_gdel_deinit(g4d_ctx* ctx);
 
-/* Batched triangulation of many clouds in one pass (persistent kernels over a
- * per-cloud work queue). xyz holds all clouds back to back; cloud c spans
- * points [cloud_offsets[c], cloud_offsets[c+1]). Tetrahedra of cloud c are
- * tets[tet_offsets[c] .. tet_offsets[c+1]) with cloud-local point indices.
+/* Batched triangulation of many clouds. The reference is one cloud per process
+ * with global state (GDelHost.cu:57-113), so this has no counterpart there; each
+ * cloud's result is the one g4d_triangulate gives at the same grid width.
+ * xyz holds all clouds back to back; cloud c spans points
+ * [cloud_offsets[c], cloud_offsets[c+1]), cloud_offsets[0] = 0, at least 5
+ * points each. Clouds are processed in passes of up to 8M points: one radix
+ * sort over all clouds of a pass, one launch per distinct grid width for the
+ * Voronoi kernels (the grids of a width are stacked), one star and splaying
+ * pipeline over all of the pass's points. Tetrahedra of cloud c are
+ * tets[tet_offsets[c] .. tet_offsets[c+1]) with cloud-local input indices.
  * *tets and *tet_offsets are library-allocated (g4d_free). */
 G4D_API g4d_status g4d_triangulate_batch(g4d_ctx* ctx, const double* xyz, const int64_t* cloud_offsets, int nclouds,
                                  g4d_tet** tets, int64_t** tet_offsets, g4d_stats* stats);
+
+/* The same with the points already on ctx's device (d_xyz, 3 doubles per
+ * point); cloud_offsets stays on the host. The tetrahedra stay in a
+ * context-owned device buffer (*d_tets) and *tet_offsets points to
+ * context-owned host offsets; both stay valid until the next batch call. */
+G4D_API g4d_status g4d_triangulate_batch_device(g4d_ctx* ctx, const double* d_xyz, const int64_t* cloud_offsets,
+                                                int nclouds, const g4d_tet** d_tets, const int64_t** tet_offsets,
+                                                g4d_stats* stats);
 
 /* Diagnostic: evaluates the device predicates on `count` point sets (host
  * arrays). kind 0: orient3d sign of 4 points (12 doubles per set);

@@ -70,6 +70,34 @@ def test_batch_fixed_grid_and_repeat_calls(oracle):
             assert np.array_equal(got[0], exp[0]) and np.array_equal(got[1], exp[1]), c
 
 
+def test_batch_autotuned_grids_match_single_calls(oracle):
+    """grid_size -1: the batch tunes a width per (size bucket, distribution
+    class); single calls on the same context reuse those widths, so every
+    cloud must still match its single-call result; the device-resident batch
+    gives the same tetrahedra."""
+    import torch
+    import gstar4d_b200
+    clouds, pts, offs = _batch(40, seed=5, hi=20000)
+    with gstar4d_b200.Triangulator(grid_size=-1) as t:
+        tets, toffs, _ = t.triangulate_batch(pts, offs)
+        d_pts = torch.from_numpy(pts).cuda()
+        dptr, ntet, doffs, _ = t.triangulate_batch_device(d_pts.data_ptr(), offs)
+        assert ntet == len(tets) and np.array_equal(doffs, toffs)
+        view = type("DeviceTets", (), {"__cuda_array_interface__": {
+            "shape": (ntet, 8), "typestr": "<i4", "data": (dptr, False), "version": 3}})()
+        dev = torch.as_tensor(view, device="cuda").cpu().numpy()
+        for c in range(len(clouds)):
+            # tetrahedron numbering follows the splaying's atomic order: compare canonical forms
+            got = oracle.canonical(dev[toffs[c]:toffs[c + 1]])
+            exp = _canon(oracle, tets[toffs[c]:toffs[c + 1]])
+            assert np.array_equal(got[0], exp[0]) and np.array_equal(got[1], exp[1]), c
+        for c, cloud in enumerate(clouds):
+            single, _, _ = t.triangulate(cloud)
+            got = _canon(oracle, tets[toffs[c]:toffs[c + 1]])
+            exp = _canon(oracle, single)
+            assert np.array_equal(got[0], exp[0]) and np.array_equal(got[1], exp[1]), c
+
+
 def test_batch_rejects_tiny_cloud():
     import gstar4d_b200
     pts = np.random.default_rng(1).random((20, 3))
