@@ -48,7 +48,7 @@ class Stats(ctypes.Structure):
                 ("drowned", ctypes.c_longlong), ("proofs", ctypes.c_longlong),
                 ("exact_predicates", ctypes.c_longlong), ("loops", ctypes.c_int), ("missing", ctypes.c_int),
                 ("grid_size", ctypes.c_int), ("tets", ctypes.c_int), ("gpu_launches", ctypes.c_longlong),
-                ("large_stars", ctypes.c_int), ("spare", ctypes.c_int)]
+                ("large_stars", ctypes.c_int), ("proposed", ctypes.c_int)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -62,7 +62,10 @@ EXPORTS = ["g4d_default_config", "g4d_create", "g4d_destroy", "g4d_last_error", 
            "g4d_triangulate", "g4d_triangulate_to", "g4d_triangulate_device", "g4d_gdel_init",
            "g4d_gdel_compute", "g4d_get_tetra", "g4d_gdel_deinit", "g4d_triangulate_batch",
            "g4d_triangulate_batch_device", "g4d_stream",
-           "g4d_eval_predicates", "g4d_voronoi", "g4d_voronoi_noalloc", "g4d_free"]
+           "g4d_eval_predicates", "g4d_voronoi", "g4d_voronoi_noalloc", "g4d_proposal_train",
+           "g4d_proposal_weights", "g4d_mlp_grad", "g4d_mlp_infer", "g4d_free"]
+
+MLP_PARAMS = 9473
 
 
 def load():
@@ -95,6 +98,11 @@ def load():
     L.g4d_eval_predicates.argtypes = [vp, ip, vp, vp, ip, vp]
     L.g4d_voronoi.argtypes = [vp, vp, ip, ip, vp]
     L.g4d_voronoi_noalloc.argtypes = [vp, ip, ip, vp, vp]
+    fp = ctypes.POINTER(ctypes.c_float)
+    L.g4d_proposal_train.argtypes = [vp, vp, ip, ip, ctypes.c_float, fp]
+    L.g4d_proposal_weights.argtypes = [vp, vp, ip, ip]
+    L.g4d_mlp_grad.argtypes = [vp, vp, vp, ip, vp, vp, fp]
+    L.g4d_mlp_infer.argtypes = [vp, vp, ip, vp, vp]
     L.g4d_stream.argtypes = [vp]
     L.g4d_stream.restype = vp
     L.g4d_free.argtypes = [vp]
@@ -207,6 +215,42 @@ class Triangulator:
         pts = np.ascontiguousarray(points, dtype=np.float64)
         out = np.empty(grid ** 3, np.uint32)
         self._check(self._lib.g4d_voronoi(self._h, _ptr(pts), len(pts), int(grid), _ptr(out)))
+        return out
+
+    # ---- learned star proposal ---------------------------------------------------------
+    def train_proposal(self, points, epochs=4, lr=2e-3):
+        """Train the proposal model on one cloud (labels from the plain method);
+        returns the last epoch's mean loss."""
+        pts = np.ascontiguousarray(points, dtype=np.float64)
+        loss = ctypes.c_float(0)
+        self._check(self._lib.g4d_proposal_train(self._h, _ptr(pts), len(pts), int(epochs), float(lr),
+                                                 ctypes.byref(loss)))
+        return loss.value
+
+    def proposal_weights(self, weights=None):
+        """Current parameters (float32[9473]); with `weights`, replace them."""
+        if weights is not None:
+            w = np.ascontiguousarray(weights, dtype=np.float32)
+            self._check(self._lib.g4d_proposal_weights(self._h, _ptr(w), len(w), 1))
+            return w
+        w = np.empty(MLP_PARAMS, np.float32)
+        self._check(self._lib.g4d_proposal_weights(self._h, _ptr(w), MLP_PARAMS, 0))
+        return w
+
+    def mlp_grad(self, x_bf16, y, params):
+        x = np.ascontiguousarray(x_bf16, dtype=np.uint16).reshape(-1, 16)
+        yy = np.ascontiguousarray(y, dtype=np.float32)
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        g = np.empty(MLP_PARAMS, np.float32)
+        loss = ctypes.c_float(0)
+        self._check(self._lib.g4d_mlp_grad(self._h, _ptr(x), _ptr(yy), len(x), _ptr(p), _ptr(g), ctypes.byref(loss)))
+        return g, loss.value
+
+    def mlp_infer(self, x_bf16, params):
+        x = np.ascontiguousarray(x_bf16, dtype=np.uint16).reshape(-1, 16)
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        out = np.empty(len(x), np.float32)
+        self._check(self._lib.g4d_mlp_infer(self._h, _ptr(x), len(x), _ptr(p), _ptr(out)))
         return out
 
     # ---- reference-shaped entry points ------------------------------------------------

@@ -16,6 +16,7 @@
 #include <cstring>
 #include <string>
 #include <map>
+#include <random>
 #include <vector>
 
 #include "g4d_internal.cuh"
@@ -51,7 +52,9 @@ enum BufId {
     B_XYZ, B_GRIDSRC, B_MM, B_KEYS, B_VALS, B_VOXIN, B_MKEY, B_ORDER, B_P, B_VOX, B_CKEY0, B_CID0, B_CKEY,
     B_CID, B_COLS, B_COLE, B_GA, B_GB, B_BUCKET, B_BCOUNT, B_HH, B_TRI, B_HDR, B_INBOX, B_ICOUNT, B_WLINS,
     B_WLEMIT, B_WLEMIT2, B_DROWN, B_DROWN2, B_CTR, B_CNT, B_BASE, B_TETS, B_CUB, B_BAD, B_LIDX, B_LHH, B_LTRI,
-    B_WLINSL, B_WLPROM, B_SKEY0, B_SKEY, B_GIDX, B_LOCAL, B_BCKEY0, B_BCKEY, B_SLOTS, B_MMB, B_TC, B_TETS2, B_OVF, B_OVF2, B_KMASK, B_BOUT, B_OCC, B_NUM
+    B_WLINSL, B_WLPROM, B_SKEY0, B_SKEY, B_GIDX, B_LOCAL, B_BCKEY0, B_BCKEY, B_SLOTS, B_MMB, B_TC, B_TETS2, B_OVF, B_OVF2, B_KMASK, B_BOUT, B_OCC,
+    B_MLP_P, B_MLP_G, B_MLP_M1, B_MLP_M2, B_MLP_AUX, B_RING_PAIR, B_RING_X, B_RING_Y, B_RING_LOGIT, B_TILES,
+    B_DIAG_X, B_DIAG_Y, B_DIAG_P, B_DIAG_G, B_NUM
 };
 
 }  // namespace
@@ -77,6 +80,11 @@ struct g4d_ctx {
     cudaEvent_t ev[8];
     std::map<int, int> tuned;  // autotuner: (size bucket, distribution class) -> grid width
     int next_grid = 0;         // tuned width for the next single-cloud call (0: none)
+    // learned star proposal
+    bool has_model = false;
+    int adam_step = 0;
+    std::vector<float> mlp;    // host copy of the parameters
+    int ring_rows = 0;         // candidate rows of the last ring pass
     std::vector<int64_t> batch_offsets;  // tet offsets of the last device batch
 };
 
@@ -306,6 +314,26 @@ g4d_status grow_ovf(g4d_ctx* ctx, Dev& D, int keep, size_t need) {
     return G4D_OK;
 }
 
+// After the worksets are formed: if the overflow request list ran out, grow it
+// and ask for the worksets to be formed again (*again).
+g4d_status worksets_fit(g4d_ctx* ctx, Dev& D, int attempt, bool* again) {
+    Counters h{};
+    CK(cudaMemcpyAsync(&h, D.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    *again = false;
+    if (h.ovf_next <= D.ovfCap) return G4D_OK;
+    if (attempt >= 2) return fail(ctx, G4D_ERR_CAPACITY, "overflow request list capacity exceeded");
+    g4d_status st = grow_ovf(ctx, D, 0, 2 * (size_t)h.ovf_next + (size_t)D.n);
+    if (st) return st;
+    CK(cudaMemsetAsync(&D.ctr->ovf_next, 0, sizeof(int), ctx->stream));
+    CK(cudaMemsetAsync(&D.ctr->proposed, 0, sizeof(int), ctx->stream));
+    h.err &= ~(unsigned)ERR_OVFCAP;
+    CK(cudaMemcpyAsync(&D.ctr->err, &h.err, sizeof(unsigned), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    *again = true;
+    return G4D_OK;
+}
+
 // Initial stars and the splaying loop (worksets already in the buckets).
 g4d_status run_splay(g4d_ctx* ctx, Dev& D) {
     Launch L{ctx->stream, &ctx->launches};
@@ -322,6 +350,7 @@ g4d_status run_splay(g4d_ctx* ctx, Dev& D) {
     CK(cudaStreamSynchronize(ctx->stream));
     g4d_status st = check_err(ctx, h.err);
     if (st) return st;
+    const unsigned long long built = h.insertions;  // initial workset insertions
     int emitCount = h.emit_next, drownCount = h.drown_next, ovfCount = h.ovf_next;
     // the lists produced by the build become the current ones
     std::swap(D.wlEmit, D.wlEmitNext);
@@ -382,9 +411,11 @@ g4d_status run_splay(g4d_ctx* ctx, Dev& D) {
     }
     cudaEventRecord(ctx->ev[4], ctx->stream);
     ctx->stats.loops = loops;
-    ctx->stats.splay_insertions = (long long)h.insertions;
+    ctx->stats.star_insertions = (long long)built;
+    ctx->stats.splay_insertions = (long long)(h.insertions - built);
     ctx->stats.proofs = (long long)h.proofs_total;
     ctx->stats.exact_predicates = (long long)h.exact;
+    ctx->stats.proposed = h.proposed;
     ctx->large_used = h.large_next;
 
     if (ctx->cfg.do_check) {
@@ -429,6 +460,74 @@ g4d_status run_extract(g4d_ctx* ctx, const Dev& D, const int* sorted_to_input) {
     return G4D_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Learned star proposal (host side)
+// ---------------------------------------------------------------------------
+
+double dkey_inv_host(unsigned long long k) {
+    const unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+    double d;
+    memcpy(&d, &b, sizeof(d));
+    return d;
+}
+
+struct MlpAux {
+    float loss;
+    unsigned err;
+    int rows;
+};
+
+// candidate rows of the 5x5x5 Voronoi block around every point, with labels
+// from the final stars when `labels`
+g4d_status run_ring(g4d_ctx* ctx, const Dev& D, bool labels) {
+    Launch L{ctx->stream, &ctx->launches};
+    const int n = D.n, G = D.G;
+    const size_t cap = 24 * (size_t)n + 1024;
+    CK(ctx->b[B_MLP_AUX].ensure(sizeof(MlpAux)));
+    CK(ctx->b[B_RING_PAIR].ensure(sizeof(int2) * cap));
+    CK(ctx->b[B_RING_X].ensure(sizeof(uint16_t) * 16 * cap));
+    CK(ctx->b[B_RING_LOGIT].ensure(sizeof(float) * cap));
+    if (labels) CK(ctx->b[B_RING_Y].ensure(sizeof(float) * cap));
+    MlpAux* aux = ctx->b[B_MLP_AUX].as<MlpAux>();
+    CK(cudaMemsetAsync(aux, 0, sizeof(MlpAux), ctx->stream));
+    // grid units per coordinate unit, as in the scaling of the points
+    unsigned long long mm[2] = {0, 0};
+    CK(cudaMemcpyAsync(mm, ctx->b[B_MM].p, sizeof(mm), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    const double range = dkey_inv_host(mm[1]) - dkey_inv_host(mm[0]);
+    Ring R;
+    R.grid = ctx->b[B_GA].as<uint32_t>();
+    R.cols = Cols<uint32_t>{D.ckey, D.cid, D.colStart, D.colEnd, G};
+    R.scale = (mm[1] && range > 0) ? (double)(G - 3) / range : 1.0;
+    R.cap = (int)cap;
+    R.rows = &aux->rows;
+    R.pair = ctx->b[B_RING_PAIR].as<int2>();
+    R.x = ctx->b[B_RING_X].as<uint16_t>();
+    R.y = labels ? ctx->b[B_RING_Y].as<float>() : nullptr;
+    launch_ring(L, D, R);
+    if (labels) launch_ring_labels(L, D, R.pair, R.rows, R.cap, R.y);
+    MlpAux h{};
+    CK(cudaMemcpyAsync(&h, aux, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->ring_rows = std::min(h.rows, R.cap);
+    return G4D_OK;
+}
+
+// score the candidates and add the accepted ones to the initial worksets
+g4d_status run_proposal(g4d_ctx* ctx, const Dev& D) {
+    if (!ctx->cfg.proposal || !ctx->has_model) return G4D_OK;
+    Launch L{ctx->stream, &ctx->launches};
+    g4d_status st = run_ring(ctx, D, false);
+    if (st) return st;
+    MlpAux* aux = ctx->b[B_MLP_AUX].as<MlpAux>();
+    if (ctx->ring_rows > 0)
+        launch_mlp_infer(L, ctx->b[B_MLP_P].as<float>(), ctx->b[B_RING_X].as<uint16_t>(), ctx->ring_rows,
+                         ctx->b[B_RING_LOGIT].as<float>(), &aux->err);
+    launch_prop_merge(L, D, ctx->b[B_RING_PAIR].as<int2>(), ctx->b[B_RING_LOGIT].as<float>(), &aux->rows,
+                      ctx->ring_rows, 0.0f);
+    return G4D_OK;
+}
+
 // Stages 2-5: digital Voronoi, stars, splaying, extraction.
 g4d_status run_compute(g4d_ctx* ctx, bool map_to_input) {
     Launch L{ctx->stream, &ctx->launches};
@@ -450,10 +549,18 @@ g4d_status run_compute(g4d_ctx* ctx, bool map_to_input) {
     launch_pba_y(L, G, gA, gB);
     launch_pba_x(L, G, gB, gA);
     cudaEventRecord(ctx->ev[2], ctx->stream);
-    // worksets
-    CK(cudaMemsetAsync(ctx->b[B_BCOUNT].p, 0, sizeof(int) * n, ctx->stream));
-    launch_pairs(L, D, gA);
-    launch_missing(L, D);
+    // worksets (repeated with a longer overflow list if theirs ran out)
+    for (int attempt = 0;; ++attempt) {
+        CK(cudaMemsetAsync(ctx->b[B_BCOUNT].p, 0, sizeof(int) * n, ctx->stream));
+        launch_pairs(L, D, gA);
+        launch_missing(L, D);
+        st = run_proposal(ctx, D);
+        if (st) return st;
+        bool again = false;
+        st = worksets_fit(ctx, D, attempt, &again);
+        if (st) return st;
+        if (!again) break;
+    }
     st = run_splay(ctx, D);
     if (st) return st;
     return run_extract(ctx, D, map_to_input ? ctx->b[B_ORDER].as<int>() : nullptr);
@@ -653,10 +760,16 @@ g4d_status run_wave(g4d_ctx* ctx, const double* d_xyz, const int64_t* offs, cons
         launch_pba_x_stack(L, S.G, S.K, gB + S.vox, gA + S.vox);
     }
     cudaEventRecord(ctx->ev[2], ctx->stream);
-    CK(cudaMemsetAsync(ctx->b[B_BCOUNT].p, 0, sizeof(int) * n, ctx->stream));
-    for (const Stack& S : stacks)
-        launch_pairs_stack(L, D, gA + S.vox, S.G, S.K, ckey, ctx->b[B_CID].as<int>(), cs + S.col, ce + S.col);
-    launch_missing_u64(L, D, skey);
+    for (int attempt = 0;; ++attempt) {
+        CK(cudaMemsetAsync(ctx->b[B_BCOUNT].p, 0, sizeof(int) * n, ctx->stream));
+        for (const Stack& S : stacks)
+            launch_pairs_stack(L, D, gA + S.vox, S.G, S.K, ckey, ctx->b[B_CID].as<int>(), cs + S.col, ce + S.col);
+        launch_missing_u64(L, D, skey);
+        bool again = false;
+        st = worksets_fit(ctx, D, attempt, &again);
+        if (st) return st;
+        if (!again) break;
+    }
     st = run_splay(ctx, D);
     if (st) return st;
     st = run_extract(ctx, D, nullptr);
@@ -854,6 +967,7 @@ g4d_status run_batch(g4d_ctx* ctx, const double* d_xyz, const int64_t* offs, int
         acc->t_star_ms += ms_between(ctx->ev[2], ctx->ev[3]);
         acc->t_splay_ms += ms_between(ctx->ev[3], ctx->ev[4]);
         acc->t_out_ms += ms_between(ctx->ev[4], ctx->ev[6]);
+        acc->star_insertions += ctx->stats.star_insertions;
         acc->splay_insertions += ctx->stats.splay_insertions;
         acc->proofs += ctx->stats.proofs;
         acc->exact_predicates += ctx->stats.exact_predicates;
@@ -1201,6 +1315,166 @@ g4d_status g4d_voronoi(g4d_ctx* ctx, const double* xyz, int n, int grid, uint32_
     launch_pba_x(L, grid, ctx->b[B_GB].as<uint32_t>(), ctx->b[B_GA].as<uint32_t>());
     CK(cudaMemcpyAsync(sites, ctx->b[B_GA].p, sizeof(uint32_t) * G3, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    return G4D_OK;
+}
+
+// ---- learned star proposal ------------------------------------------------
+
+static g4d_status mlp_upload(g4d_ctx* ctx) {
+    CK(ctx->b[B_MLP_P].ensure(sizeof(float) * MLP_NPARAMS));
+    CK(ctx->b[B_MLP_G].ensure(sizeof(float) * MLP_NPARAMS));
+    CK(ctx->b[B_MLP_M1].ensure(sizeof(float) * MLP_NPARAMS));
+    CK(ctx->b[B_MLP_M2].ensure(sizeof(float) * MLP_NPARAMS));
+    CK(cudaMemcpyAsync(ctx->b[B_MLP_P].p, ctx->mlp.data(), sizeof(float) * MLP_NPARAMS, cudaMemcpyHostToDevice,
+                       ctx->stream));
+    CK(cudaMemsetAsync(ctx->b[B_MLP_G].p, 0, sizeof(float) * MLP_NPARAMS, ctx->stream));
+    CK(cudaMemsetAsync(ctx->b[B_MLP_M1].p, 0, sizeof(float) * MLP_NPARAMS, ctx->stream));
+    CK(cudaMemsetAsync(ctx->b[B_MLP_M2].p, 0, sizeof(float) * MLP_NPARAMS, ctx->stream));
+    ctx->adam_step = 0;
+    ctx->has_model = true;
+    return G4D_OK;
+}
+
+// He-uniform initialisation (fixed seed), zero biases
+static void mlp_init(std::vector<float>& w) {
+    w.assign(MLP_NPARAMS, 0.f);
+    std::mt19937 rng(20240611u);
+    auto fill = [&](int off, int count, int fan_in, float gain) {
+        std::uniform_real_distribution<float> u(-1.f, 1.f);
+        const float a = gain * std::sqrt(6.f / (float)fan_in);
+        for (int i = 0; i < count; ++i) w[off + i] = a * u(rng);
+    };
+    fill(0, 64 * 16, 6, 1.f);                     // W1 (6 live inputs)
+    fill(64 * 16 + 64, 64 * 64, 64, 1.f);         // W2
+    fill(64 * 16 + 64 + 64 * 64 + 64, 64 * 64, 64, 1.f);  // W3
+    fill(64 * 16 + 64 + 2 * (64 * 64 + 64), 64, 64, 0.1f);  // w4
+}
+
+g4d_status g4d_proposal_train(g4d_ctx* ctx, const double* xyz, int n, int epochs, float lr, float* loss_out) {
+    g4d_status st = check_n(ctx, n);
+    if (st) return st;
+    if (!xyz || epochs < 0 || !(lr > 0.f)) return fail(ctx, G4D_ERR_ARG, "bad training arguments");
+    cudaSetDevice(ctx->device);
+    // labels come from the plain method
+    const int saved = ctx->cfg.proposal;
+    ctx->cfg.proposal = 0;
+    CK(ctx->b[B_XYZ].ensure(sizeof(double) * 3 * (size_t)n));
+    CK(cudaMemcpyAsync(ctx->b[B_XYZ].p, xyz, sizeof(double) * 3 * (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
+    st = run_all_device(ctx, ctx->b[B_XYZ].as<double>(), nullptr, n, false);
+    ctx->cfg.proposal = saved;
+    if (st) return st;
+    Dev D = make_dev(ctx);
+    D.anyLarge = ctx->large_used > 0;
+    st = run_ring(ctx, D, true);
+    if (st) return st;
+    if (!ctx->has_model) {
+        mlp_init(ctx->mlp);
+        st = mlp_upload(ctx);
+        if (st) return st;
+    }
+    const int M = ctx->ring_rows;
+    const int ntiles = (M + 127) / 128;
+    const int per_step = 64;  // tiles per optimizer step (8192 rows)
+    Launch L{ctx->stream, &ctx->launches};
+    MlpAux* aux = ctx->b[B_MLP_AUX].as<MlpAux>();
+    CK(ctx->b[B_TILES].ensure(sizeof(int) * std::max(ntiles, 1)));
+    std::vector<int> order(ntiles);
+    std::mt19937 rng(7u + (unsigned)ctx->adam_step);
+    float last = 0.f;
+    for (int ep = 0; ep < epochs; ++ep) {
+        for (int i = 0; i < ntiles; ++i) order[i] = i;
+        std::shuffle(order.begin(), order.end(), rng);
+        CK(cudaMemcpyAsync(ctx->b[B_TILES].p, order.data(), sizeof(int) * ntiles, cudaMemcpyHostToDevice,
+                           ctx->stream));
+        CK(cudaMemsetAsync(aux, 0, sizeof(MlpAux), ctx->stream));
+        for (int b0 = 0; b0 < ntiles; b0 += per_step) {
+            const int nb = std::min(per_step, ntiles - b0);
+            int rows = 0;
+            for (int i = b0; i < b0 + nb; ++i) rows += std::min(128, M - 128 * order[i]);
+            launch_mlp_train(L, ctx->b[B_MLP_P].as<float>(), ctx->b[B_RING_X].as<uint16_t>(),
+                             ctx->b[B_RING_Y].as<float>(), M, ctx->b[B_TILES].as<int>() + b0, nb, 1.f / (float)rows,
+                             ctx->b[B_MLP_G].as<float>(), &aux->loss, &aux->err);
+            launch_adam(L, ctx->b[B_MLP_P].as<float>(), ctx->b[B_MLP_G].as<float>(), ctx->b[B_MLP_M1].as<float>(),
+                        ctx->b[B_MLP_M2].as<float>(), ++ctx->adam_step, lr);
+        }
+        MlpAux h{};
+        CK(cudaMemcpyAsync(&h, aux, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        if (h.err) return fail(ctx, G4D_ERR_INTERNAL, "tensor-core training kernel timed out waiting (0x%x)", h.err);
+        last = M ? h.loss / (float)M : 0.f;
+    }
+    CK(cudaMemcpyAsync(ctx->mlp.data(), ctx->b[B_MLP_P].p, sizeof(float) * MLP_NPARAMS, cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (loss_out) *loss_out = last;
+    return G4D_OK;
+}
+
+g4d_status g4d_proposal_weights(g4d_ctx* ctx, float* w, int count, int set) {
+    if (!ctx) return G4D_ERR_ARG;
+    if (!w || count != MLP_NPARAMS)
+        return fail(ctx, G4D_ERR_ARG, "the proposal model has %d parameters (got %d)", MLP_NPARAMS, count);
+    cudaSetDevice(ctx->device);
+    if (set) {
+        ctx->mlp.assign(w, w + MLP_NPARAMS);
+        g4d_status st = mlp_upload(ctx);
+        if (st) return st;
+        CK(cudaStreamSynchronize(ctx->stream));
+        return G4D_OK;
+    }
+    if (!ctx->has_model) return fail(ctx, G4D_ERR_ARG, "no proposal model (train or set one first)");
+    memcpy(w, ctx->mlp.data(), sizeof(float) * MLP_NPARAMS);
+    return G4D_OK;
+}
+
+// diagnostic: one pass of the training kernel (no update) on given rows
+g4d_status g4d_mlp_grad(g4d_ctx* ctx, const uint16_t* x, const float* y, int m, const float* params, float* grads,
+                        float* loss) {
+    if (!ctx || !x || !y || m < 1 || !params || !grads) return G4D_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    CK(ctx->b[B_DIAG_X].ensure(sizeof(uint16_t) * 16 * (size_t)m));
+    CK(ctx->b[B_DIAG_Y].ensure(sizeof(float) * (size_t)m));
+    CK(ctx->b[B_DIAG_P].ensure(sizeof(float) * MLP_NPARAMS));
+    CK(ctx->b[B_DIAG_G].ensure(sizeof(float) * MLP_NPARAMS));
+    CK(ctx->b[B_MLP_AUX].ensure(sizeof(MlpAux)));
+    CK(cudaMemcpyAsync(ctx->b[B_DIAG_X].p, x, sizeof(uint16_t) * 16 * (size_t)m, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->b[B_DIAG_Y].p, y, sizeof(float) * (size_t)m, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->b[B_DIAG_P].p, params, sizeof(float) * MLP_NPARAMS, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemsetAsync(ctx->b[B_DIAG_G].p, 0, sizeof(float) * MLP_NPARAMS, ctx->stream));
+    MlpAux* aux = ctx->b[B_MLP_AUX].as<MlpAux>();
+    CK(cudaMemsetAsync(aux, 0, sizeof(MlpAux), ctx->stream));
+    Launch L{ctx->stream, &ctx->launches};
+    launch_mlp_train(L, ctx->b[B_DIAG_P].as<float>(), ctx->b[B_DIAG_X].as<uint16_t>(), ctx->b[B_DIAG_Y].as<float>(),
+                     m, nullptr, (m + 127) / 128, 1.f / (float)m, ctx->b[B_DIAG_G].as<float>(), &aux->loss, &aux->err);
+    MlpAux h{};
+    CK(cudaMemcpyAsync(grads, ctx->b[B_DIAG_G].p, sizeof(float) * MLP_NPARAMS, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(&h, aux, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (h.err) return fail(ctx, G4D_ERR_INTERNAL, "tensor-core training kernel timed out waiting (0x%x)", h.err);
+    if (loss) *loss = h.loss / (float)m;
+    return G4D_OK;
+}
+
+// diagnostic: logits of given rows
+g4d_status g4d_mlp_infer(g4d_ctx* ctx, const uint16_t* x, int m, const float* params, float* logits) {
+    if (!ctx || !x || m < 1 || !params || !logits) return G4D_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    CK(ctx->b[B_DIAG_X].ensure(sizeof(uint16_t) * 16 * (size_t)m));
+    CK(ctx->b[B_DIAG_Y].ensure(sizeof(float) * (size_t)m));
+    CK(ctx->b[B_DIAG_P].ensure(sizeof(float) * MLP_NPARAMS));
+    CK(ctx->b[B_MLP_AUX].ensure(sizeof(MlpAux)));
+    CK(cudaMemcpyAsync(ctx->b[B_DIAG_X].p, x, sizeof(uint16_t) * 16 * (size_t)m, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->b[B_DIAG_P].p, params, sizeof(float) * MLP_NPARAMS, cudaMemcpyHostToDevice, ctx->stream));
+    MlpAux* aux = ctx->b[B_MLP_AUX].as<MlpAux>();
+    CK(cudaMemsetAsync(aux, 0, sizeof(MlpAux), ctx->stream));
+    Launch L{ctx->stream, &ctx->launches};
+    launch_mlp_infer(L, ctx->b[B_DIAG_P].as<float>(), ctx->b[B_DIAG_X].as<uint16_t>(), m,
+                     ctx->b[B_DIAG_Y].as<float>(), &aux->err);
+    MlpAux h{};
+    CK(cudaMemcpyAsync(logits, ctx->b[B_DIAG_Y].p, sizeof(float) * (size_t)m, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(&h, aux, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (h.err) return fail(ctx, G4D_ERR_INTERNAL, "tensor-core inference kernel timed out waiting (0x%x)", h.err);
     return G4D_OK;
 }
 

@@ -8,7 +8,7 @@
 //                           star (bit 31 = currently in the link), open addressing
 //   tri      uint2[n*224]   per-star link triangles, 8 bytes each (packing below)
 //   lhh/ltri                the same for the few stars promoted to the large class
-//                           (2048 hash slots, 1024 triangles of 16 bytes)
+//                           (4096 hash slots, 2048 triangles of 16 bytes)
 //   hdr      StarHdr[n]     triangle count, history count, pass number, flags
 //   bucket   int32[n*64]    initial candidate worksets (Voronoi pairs + missing)
 //   inbox    int32[n*64]    insertion requests for the next splaying round
@@ -42,10 +42,10 @@ constexpr int HSLOTS = 512;               // small: history hash slots per star
 constexpr int HMAX = 255;                 // small: max history entries (hash load <= 1/2)
 constexpr int TMAX = 220;                 // small: max link triangles (a link of 112 points)
 constexpr int TSTRIDE = 224;              // small: triangle slots per star in HBM
-constexpr int LHSLOTS = 2048;             // large: history hash slots
-constexpr int LHMAX = 1023;               // large: max history entries
-constexpr int LTMAX = 1020;               // large: max link triangles
-constexpr int LTSTRIDE = 1024;            // large: triangle slots in HBM
+constexpr int LHSLOTS = 4096;             // large: history hash slots
+constexpr int LHMAX = 2047;               // large: max history entries
+constexpr int LTMAX = 2044;               // large: max link triangles
+constexpr int LTSTRIDE = 2048;            // large: triangle slots in HBM
 constexpr int BUCKET_CAP = 64;            // initial candidates kept per star
 constexpr int INBOX_CAP = 64;             // insertion requests per star per round
 constexpr int MIN_WORKSET = 8;            // GDelCommon.h:49
@@ -88,6 +88,7 @@ struct Counters {
     unsigned long long drowned_total;
     unsigned long long proofs_total;
     int tet_count;
+    int proposed;         // candidate pairs the learned proposal added
     int dbg_set;          // first failing exact-predicate input recorded below
     double dbg_pts[15];
     int dbg_ids[5];
@@ -164,6 +165,40 @@ struct Dev {
     int nclouds;
 };
 
+// column-sorted sites of one grid of a stack
+template <class KeyT>
+struct Cols {
+    const KeyT* key;   // (column << 10) | z, sorted
+    const int* cid;    // point id of each key
+    const int* start;  // first key of each column of this grid
+    const int* end;
+    int G;
+};
+
+// site (packed voxel) -> point id of the voxel's leader (smallest Morton index)
+template <class KeyT>
+__device__ __forceinline__ int site_to_id(const Cols<KeyT>& C, uint32_t e) {
+    const int c = (int)(vy(e) * (uint32_t)C.G + vx(e));
+    const uint32_t z = vz(e);
+    for (int j = C.start[c], je = C.end[c]; j < je; ++j)
+        if ((uint32_t)(C.key[j] & 1023u) == z) return C.cid[j];
+    return -1;
+}
+
+// Initial workset entry b of point a. Worksets are symmetric (b in a's <=> a in
+// b's), which splaying relies on; an entry that finds a's workset full becomes
+// an insertion request sent after the initial stars are built.
+__device__ __forceinline__ void bucket_push(const Dev& D, int a, int b) {
+    const int pos = atomicAdd(&D.bucketCount[a], 1);
+    if (pos < BUCKET_CAP) {
+        D.bucket[(size_t)a * BUCKET_CAP + pos] = b;
+        return;
+    }
+    const int q = atomicAdd(&D.ctr->ovf_next, 1);
+    if (q < D.ovfCap) D.ovfNext[q] = make_int2(a, b);
+    else atomicOr(&D.ctr->err, ERR_OVFCAP);
+}
+
 // ---- launchers (host) --------------------------------------------------------
 struct Launch {
     cudaStream_t stream;
@@ -220,6 +255,28 @@ void launch_proof(const Launch& L, const Dev& D, int count);
 void launch_check(const Launch& L, const Dev& D, unsigned long long* bad);
 void launch_tet_count(const Launch& L, const Dev& D, int* cnt);
 void launch_tet_write(const Launch& L, const Dev& D, const int* base, g4d_tet* tets, const int* sorted_to_input);
+// learned star proposal (g4d_mlp.cu, g4d_proposal.cu)
+constexpr int MLP_NPARAMS = 9473;
+size_t mlp_infer_smem();
+size_t mlp_train_smem();
+void launch_mlp_infer(const Launch& L, const float* P, const uint16_t* X, int M, float* logits, unsigned* err);
+void launch_mlp_train(const Launch& L, const float* P, const uint16_t* X, const float* Y, int M, const int* tiles,
+                      int ntiles, float inv_batch, float* G, float* loss, unsigned* err);
+void launch_adam(const Launch& L, float* P, float* G, float* m1, float* m2, int step, float lr);
+struct Ring {
+    const uint32_t* grid;  // Voronoi sites of the cloud's grid
+    Cols<uint32_t> cols;
+    double scale;          // grid units per coordinate unit
+    int cap;               // rows available
+    int* rows;             // row counter
+    int2* pair;            // [cap] (star, candidate)
+    uint16_t* x;           // [cap * 16] BF16 features
+    float* y;              // [cap] labels (final Delaunay edge), or null
+};
+void launch_ring(const Launch& L, const Dev& D, const Ring& R);
+void launch_ring_labels(const Launch& L, const Dev& D, const int2* pair, const int* rows, int cap, float* y);
+void launch_prop_merge(const Launch& L, const Dev& D, const int2* pair, const float* logits, const int* rows,
+                       int cap, float threshold);
 void launch_eval_pred(const Launch& L, int kind, const double* pts, const int* idx, int count, int8_t* out,
                       unsigned* err);
 

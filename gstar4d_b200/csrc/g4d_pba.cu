@@ -148,30 +148,6 @@ __global__ void __launch_bounds__(256) k_pba_x(int G, const uint32_t* __restrict
     }
 }
 
-// column-sorted sites of one grid of a stack
-template <class KeyT>
-struct Cols {
-    const KeyT* key;   // (column << 10) | z, sorted
-    const int* cid;    // point id of each key
-    const int* start;  // first key of each column of this grid
-    const int* end;
-    int G;
-};
-
-// site (packed voxel) -> point id of the voxel's leader (smallest Morton index)
-template <class KeyT>
-__device__ __forceinline__ int site_to_id(const Cols<KeyT>& C, uint32_t e) {
-    const int c = (int)(vy(e) * (uint32_t)C.G + vx(e));
-    const uint32_t z = vz(e);
-    for (int j = C.start[c], je = C.end[c]; j < je; ++j)
-        if ((uint32_t)(C.key[j] & 1023u) == z) return C.cid[j];
-    return -1;
-}
-
-__device__ __forceinline__ void push_bucket(const Dev& D, int a, int b) {
-    const int pos = atomicAdd(&D.bucketCount[a], 1);
-    if (pos < BUCKET_CAP) D.bucket[(size_t)a * BUCKET_CAP + pos] = b;
-}
 
 constexpr int PAIR_HASH = 4096;
 constexpr int PAIR_PROBES = 32;
@@ -189,7 +165,7 @@ __device__ __forceinline__ void pair_hash_insert(unsigned long long* hs, unsigne
     // crowded table (dense regions hold thousands of pairs per block): emit
     // directly instead of probing further
     const int ia = site_to_id(C, (uint32_t)(key >> 32)), ib = site_to_id(C, (uint32_t)key);
-    if (ia >= 0 && ib >= 0) { push_bucket(D, ia, ib); push_bucket(D, ib, ia); }
+    if (ia >= 0 && ib >= 0) { bucket_push(D, ia, ib); bucket_push(D, ib, ia); }
 }
 
 // Candidate Delaunay edges: every two distinct sites of a 2x2x2 voxel cube in
@@ -264,8 +240,8 @@ __global__ void __launch_bounds__(128) k_pairs(Dev D, const uint32_t* __restrict
         if (key == ~0ull) continue;
         const int ia = site_to_id(C, (uint32_t)(key >> 32)), ib = site_to_id(C, (uint32_t)key);
         if (ia >= 0 && ib >= 0) {
-            push_bucket(D, ia, ib);
-            push_bucket(D, ib, ia);
+            bucket_push(D, ia, ib);
+            bucket_push(D, ib, ia);
         }
     }
 }
@@ -279,8 +255,8 @@ __global__ void k_missing(Dev D, const KeyT* __restrict__ mkey) {
         if (i == 0 || mkey[i - 1] != k) continue;
         int j = i - 1;
         while (j > 0 && mkey[j - 1] == k) --j;
-        push_bucket(D, i, j);
-        push_bucket(D, j, i);
+        bucket_push(D, i, j);
+        bucket_push(D, j, i);
     }
 }
 

@@ -17,7 +17,7 @@
 // points, 252 triangles, 4 KB in HBM, 16 KB of shared memory while a warp works
 // on it) that fits nearly every star; a star that outgrows it during a round is
 // left untouched, its inbox kept, and k_promote copies it to a large slot
-// (1023 points, 1020 triangles) before the large-class kernel replays the
+// (2047 points, 2044 triangles) before the large-class kernel replays the
 // round's insertions for it. lidx[s] says which class holds star s.
 #include "g4d_internal.cuh"
 #include "g4d_predicates.cuh"
@@ -60,19 +60,19 @@ struct SmallStar {
 //   x = v0 | v1<<16, y = v2 | gen<<16 | kept<<31, z = o0 | o1<<16,
 //   w = o2 | j0<<16 | j1<<18 | j2<<20
 struct LargeStar {
-    static constexpr int LOG2_HS = 11, HS = LHSLOTS, HM = LHMAX, TM = LTMAX, TS = LTSTRIDE;
-    static constexpr int WARPS = 1, MINB = 2;  // about 80 KB of shared memory per warp
+    static constexpr int LOG2_HS = 12, HS = LHSLOTS, HM = LHMAX, TM = LTMAX, TS = LTSTRIDE;
+    static constexpr int WARPS = 1, MINB = 1;  // about 141 KB of shared memory per warp
     static constexpr bool LARGE = true;
     using Idx = uint16_t;
-    using Rec = unsigned long long;  // u | w<<11 | o<<22 | oj<<32
+    using Rec = unsigned long long;  // u | w<<12 | o<<24 | oj<<35
     using Tri = uint4;
     __device__ static Rec rec(int u, int w, int o, int oj) {
-        return (Rec)u | ((Rec)w << 11) | ((Rec)o << 22) | ((Rec)oj << 32);
+        return (Rec)u | ((Rec)w << 12) | ((Rec)o << 24) | ((Rec)oj << 35);
     }
-    __device__ static int rec_u(Rec e) { return (int)(e & 2047u); }
-    __device__ static int rec_w(Rec e) { return (int)((e >> 11) & 2047u); }
-    __device__ static int rec_o(Rec e) { return (int)((e >> 22) & 1023u); }
-    __device__ static int rec_oj(Rec e) { return (int)((e >> 32) & 3u); }
+    __device__ static int rec_u(Rec e) { return (int)(e & 4095u); }
+    __device__ static int rec_w(Rec e) { return (int)((e >> 12) & 4095u); }
+    __device__ static int rec_o(Rec e) { return (int)((e >> 24) & 2047u); }
+    __device__ static int rec_oj(Rec e) { return (int)((e >> 35) & 3u); }
     __device__ static int tv(Tri T, int i) {
         return (int)(i == 0 ? (T.x & 0xffffu) : (i == 1 ? (T.x >> 16) : (T.y & 0xffffu)));
     }
@@ -95,7 +95,7 @@ struct LargeStar {
 };
 
 // Per-warp shared-memory image of one star (14 KB small, so that 16 warps fit
-// on an SM; 76 KB large).
+// on an SM; 141 KB large).
 template <class C>
 struct WS {
     using Idx = typename C::Idx;
@@ -121,6 +121,7 @@ struct WS {
 
 // 4 blocks of 4 warps per SM: 16 images plus the per-block reservation in 228 KB
 static_assert(4 * (4 * sizeof(WS<SmallStar>) + 1024) <= 228 * 1024, "small star image too large");
+static_assert(sizeof(WS<LargeStar>) + 1024 <= 227 * 1024, "large star image too large");
 
 // Read-only view of any star, whichever class holds it (cross-star lookups).
 struct StarView {
@@ -1195,7 +1196,23 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_tet_write(Dev D, const
     }
 }
 
+// training labels of the learned proposal: (s, v) is an edge of the final
+// triangulation when v is in the final link of s
+__global__ void k_ring_labels(Dev D, const int2* __restrict__ pair, const int* __restrict__ rows, int cap,
+                              float* __restrict__ y) {
+    const int n = min(*rows, cap);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        y[i] = hist_state(D, pair[i].x, pair[i].y) == 2 ? 1.f : 0.f;
+}
+
 #ifndef G4D_HOST_EMULATION
+void launch_ring_labels(const Launch& L, const Dev& D, const int2* pair, const int* rows, int cap, float* y) {
+    int b = (cap + 255) / 256;
+    if (b > 148 * 8) b = 148 * 8;
+    k_ring_labels<<<b < 1 ? 1 : b, 256, 0, L.stream>>>(D, pair, rows, cap, y);
+    ++*L.launches;
+}
+
 // --------------------------------------------------------------------------
 // diagnostic predicate evaluation
 // --------------------------------------------------------------------------
@@ -1270,7 +1287,7 @@ void launch_star_insert(const Launch& L, const Dev& D, int count) {
 void launch_star_insert_large(const Launch& L, const Dev& D, const int* list, int count) {
     const size_t sm = sizeof(WS<LargeStar>) * LargeStar::WARPS;
     cudaFuncSetAttribute(k_star_insert<LargeStar>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_star_insert<LargeStar><<<star_blocks(count, LargeStar::WARPS, 2), 32 * LargeStar::WARPS, sm, L.stream>>>(
+    k_star_insert<LargeStar><<<star_blocks(count, LargeStar::WARPS, 1), 32 * LargeStar::WARPS, sm, L.stream>>>(
         D, list, count);
     ++*L.launches;
 }

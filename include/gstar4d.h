@@ -86,7 +86,7 @@ typedef struct {
     int tets;
     long long gpu_launches;      /* kernels launched by this call */
     int large_stars;             /* stars that outgrew the small storage class */
-    int spare;
+    int proposed;                /* candidate pairs the learned proposal added */
 } g4d_stats;
 
 typedef struct g4d_ctx g4d_ctx;
@@ -183,6 +183,27 @@ G4D_API g4d_status g4d_voronoi(g4d_ctx* ctx, const double* xyz, int n, int grid,
  * race and must be serialized by the caller. The first call on each device
  * looks up the array's address; make it outside any stream capture. */
 G4D_API g4d_status g4d_voronoi_noalloc(const double* d_xyz, int n, int grid, uint32_t* d_sites, void* stream);
+
+/* Learned star proposal (no counterpart in the reference). A BF16 MLP scores
+ * candidate pairs (s, v) from the 5x5x5 block of the digital Voronoi grid around
+ * each point; with config.proposal = 1 the accepted pairs join the initial
+ * worksets. Splaying with exact predicates still decides every star, so the
+ * tetrahedra do not change; only the splaying work does.
+ * g4d_proposal_train: triangulates xyz with the plain method, labels every
+ * candidate pair by whether it is an edge of the result, and trains the model
+ * on the device for `epochs` passes (Adam, learning rate lr; a new context starts
+ * from a fixed-seed initialisation, later calls continue). *loss receives the
+ * last pass's mean binary cross-entropy. */
+G4D_API g4d_status g4d_proposal_train(g4d_ctx* ctx, const double* xyz, int n, int epochs, float lr, float* loss);
+/* Read (set = 0) or replace (set = 1) the 9473 FP32 model parameters:
+ * W1[64][16], b1[64], W2[64][64], b2[64], W3[64][64], b3[64], w4[64], b4. */
+G4D_API g4d_status g4d_proposal_weights(g4d_ctx* ctx, float* w, int count, int set);
+/* Diagnostics of the tensor-core kernels on given rows (x: m rows of 16 BF16
+ * features as uint16, y: labels): gradients of the mean loss with respect to
+ * `params` (one training-kernel pass, no update), and logits. */
+G4D_API g4d_status g4d_mlp_grad(g4d_ctx* ctx, const uint16_t* x, const float* y, int m, const float* params,
+                                float* grads, float* loss);
+G4D_API g4d_status g4d_mlp_infer(g4d_ctx* ctx, const uint16_t* x, int m, const float* params, float* logits);
 
 /* The context's CUDA stream (a cudaStream_t), for callers that time or order
  * their own work against the library's launches. */

@@ -86,6 +86,21 @@ def test_parity_degenerate500k_with_large_stars(oracle):
     assert np.array_equal(g[1], r[1]), "adjacency differs"
 
 
+def test_parity_dense_voxels_overflow_worksets(oracle):
+    """Tight clusters on a coarse grid: dozens of points share a voxel, so the
+    voxel leaders' initial worksets overflow their 64 slots; the overflowing
+    entries must still reach both points (symmetric worksets), or splaying
+    stops with inconsistent stars."""
+    import gstar4d_b200
+    pts = workloads.clustered(30000, k=4, sigma=0.03, seed=9, uniform_frac=0.1)
+    with gstar4d_b200.Triangulator(grid_size=64, do_check=1) as t:
+        tets, _, _ = t.triangulate(pts)
+    ref, _, _ = oracle.triangulate(pts, 64)
+    g, r = _canon(oracle, tets), oracle.canonical(ref)
+    assert np.array_equal(g[0], r[0]), "tetrahedra differ"
+    assert np.array_equal(g[1], r[1]), "adjacency differs"
+
+
 def test_morton_index_space_and_gdel_entry_points(oracle):
     """gdelInit/gdelCompute/getTetraFromGpu shape: points already in grid units,
     overwritten with the Morton order; output in Morton indices."""

@@ -124,3 +124,26 @@ def test_oracle_grid_size_does_not_change_result(oracle):
         assert np.array_equal(oracle.canonical(a)[0], oracle.canonical(b)[0])
     # generic points: no exact degeneracy, so the mesh is the plain Delaunay mesh
     assert np.array_equal(oracle.canonical(a)[0], oracle.canonical(b)[0])
+
+
+def test_mlp_oracle_gradient_matches_finite_differences():
+    """The FP64 network restatement (the checker of the tensor-core training
+    kernel): analytic gradient of the unrounded function vs central
+    differences, on a few coordinates of every parameter block."""
+    from oracle import mlp_oracle as mo
+    _, x = mo.sample_rows(40, seed=3)
+    y = (np.random.default_rng(4).random(40) < 0.5).astype(np.float64)
+    p = mo.init_params(seed=5)
+    _, g, _ = mo.forward_backward(x, y, p, rounding=False)
+    rng = np.random.default_rng(6)
+    blocks = [(mo.P_W1, mo.P_B1), (mo.P_B1, mo.P_W2), (mo.P_W2, mo.P_B2), (mo.P_B2, mo.P_W3), (mo.P_W3, mo.P_B3),
+              (mo.P_B3, mo.P_W4), (mo.P_W4, mo.P_B4), (mo.P_B4, mo.NPARAMS)]
+    for lo, hi in blocks:
+        live = [i for i in range(lo, hi) if not (lo == mo.P_W1 and (i - lo) % 16 >= 6)]
+        for i in rng.choice(live, size=min(4, len(live)), replace=False):
+            h = 1e-6
+            pp, pm = p.copy(), p.copy()
+            pp[i] += h
+            pm[i] -= h
+            fd = (mo.forward_backward(x, y, pp, rounding=False)[0] - mo.forward_backward(x, y, pm, rounding=False)[0]) / (2 * h)
+            assert abs(fd - g[i]) <= 1e-6 + 1e-4 * abs(g[i]), (i, fd, g[i])
