@@ -252,6 +252,7 @@ def main():
     ap.add_argument("--points", type=int, default=None)
     ap.add_argument("--grid", type=int, default=None)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-learned", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -317,6 +318,49 @@ def main():
         total_ms = float(t.item())
     value = world * n * args.steps / (total_ms / 1e3) / 1e6
 
+    # ---- learned star proposal: trained (untimed) on another seeded cloud of the
+    # same distribution with labels from the plain method, then timed like value
+    learned = None
+    if not args.no_learned:
+        train_pts, _ = workloads.config_cloud(args.workload, scale=args.points / WORKLOADS[args.workload]["points"],
+                                              seed=cfg["seed"] + 1000 + rank)
+        with gstar4d_b200.Triangulator(grid_size=args.grid, device=local) as tt:
+            t0 = time.perf_counter()
+            loss = tt.train_proposal(train_pts, epochs=4, lr=2e-3)
+            train_s = time.perf_counter() - t0
+            weights = tt.proposal_weights()
+        tl = gstar4d_b200.Triangulator(grid_size=args.grid, device=local, proposal=1)
+        tl.proposal_weights(weights)
+        extl = torch.cuda.ExternalStream(tl.stream, device=local)
+        for _ in range(args.warmup):
+            tl.triangulate_device(d_pts.data_ptr(), n)
+        barrier()
+        lms = []
+        for _ in range(args.steps):
+            flush.fill_(1)
+            torch.cuda.synchronize()
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(extl)
+            _, ntl, stl = tl.triangulate_device(d_pts.data_ptr(), n)
+            e.record(extl)
+            e.synchronize()
+            lms.append(s.elapsed_time(e))
+        barrier()
+        lt = sum(lms)
+        if world > 1:
+            tt_ = torch.tensor([lt], device=f"cuda:{local}")
+            dist.all_reduce(tt_, op=dist.ReduceOp.MAX)
+            lt = float(tt_.item())
+        learned = {"value": round(world * n * args.steps / (lt / 1e3) / 1e6, 3), "unit": "Mpts/s",
+                   "ms_per_step": round(lt / args.steps, 3), "tets": ntl,
+                   "star_insertions_per_point": round(stl["star_insertions"] / n, 3),
+                   "splay_insertions_per_point": round(stl["splay_insertions"] / n, 3),
+                   "proposed_per_point": round(stl["proposed"] / n, 3), "loops": stl["loops"],
+                   "stages_ms": {k: round(stl[k], 3) for k in ("t_pba_ms", "t_star_ms", "t_splay_ms", "t_out_ms")},
+                   "training": {"cloud": "same distribution, seed + 1000", "epochs": 4, "final_loss": round(loss, 4),
+                                "seconds": round(train_s, 2)}}
+        tl.close()
+
     # ---- end to end through the public API with pinned host buffers ----
     h_pts = torch.from_numpy(pts).pin_memory()
     cap = int(ntets * 1.2) + 1024
@@ -361,9 +405,11 @@ def main():
                          "traffic": None, "algorithmic_bytes": alg_bytes, "avg_ms": round(pba_avg, 4)},
             "stages_ms": {k: round(last[k], 3) for k in ("t_init_ms", "t_pba_ms", "t_star_ms", "t_splay_ms",
                                                           "t_out_ms", "t_total_ms")},
-            "splay": {"loops": last["loops"], "insertions": last["splay_insertions"], "proofs": last["proofs"],
-                      "exact_predicates": last["exact_predicates"], "large_stars": last["large_stars"],
-                      "tets": ntets},
+            "splay": {"loops": last["loops"], "star_insertions_per_point": round(last["star_insertions"] / n, 3),
+                      "splay_insertions_per_point": round(last["splay_insertions"] / n, 3),
+                      "proofs": last["proofs"], "exact_predicates": last["exact_predicates"],
+                      "large_stars": last["large_stars"], "tets": ntets},
+            "learned_proposal": learned,
             "clocks": clocks,
             "gpu_launches": int(launches),
         }

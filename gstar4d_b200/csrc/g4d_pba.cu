@@ -169,9 +169,9 @@ __device__ __forceinline__ void pair_hash_insert(unsigned long long* hs, unsigne
 }
 
 // Candidate Delaunay edges: every two distinct sites of a 2x2x2 voxel cube in
-// which at least three sites meet (a digital Voronoi edge or vertex; the
-// reference reads the same cubes and emits around digital Voronoi vertices,
-// GDelKernels.cu:137-299). One thread sweeps a column of cubes along z,
+// which at least four sites meet (a digital Voronoi vertex: its sites are
+// pairwise Voronoi neighbours; the reference reads the same cubes and emits
+// around digital Voronoi vertices, GDelKernels.cu:137-299). One thread sweeps a column of cubes along z,
 // keeping the previous voxel plane in registers (4 new loads per cube,
 // coalesced over x); a per-thread cache of the last pairs and a block-local
 // hash remove duplicates before the per-star scatter.
@@ -213,7 +213,7 @@ __global__ void __launch_bounds__(128) k_pairs(Dev D, const uint32_t* __restrict
                 for (int k = 0; k < ns; ++k) dup |= (s[k] == v[i]);
                 if (!dup) s[ns++] = v[i];
             }
-            const int np = (active && ns >= 3) ? ns * (ns - 1) / 2 : 0;
+            const int np = (active && ns >= 4) ? ns * (ns - 1) / 2 : 0;
             const int maxp = __reduce_max_sync(0xffffffffu, (unsigned)np);
             int pi = 0, pj = 1;
             for (int k = 0; k < maxp; ++k) {
