@@ -23,6 +23,10 @@
 
 namespace g4d {
 
+#ifndef PBA_U
+#define PBA_U 2  // search distances per loop iteration in the y and x passes
+#endif
+
 template <class KeyT>
 __global__ void __launch_bounds__(128) k_pba_z(int G, const KeyT* __restrict__ ckey, const int* __restrict__ cs,
                                                const int* __restrict__ ce, uint32_t* __restrict__ out) {
@@ -73,27 +77,25 @@ __global__ void __launch_bounds__(256) k_pba_y(int G, const uint32_t* __restrict
     for (int k = threadIdx.x; k < total; k += blockDim.x) {
         const int xx = k / G, y = k % G;
         const uint32_t* line = lines + xx * (G + 1);
-        uint32_t best = MARKER;
-        int bestd = 0x7fffffff;
-        for (int d = 0;; ++d) {
-            if (d * d >= bestd) break;
-            const int ya = y - d, yb = y + d;
-            if (ya < 0 && yb >= G) break;
-            if (ya >= 0) {
-                const uint32_t s = line[ya];
-                if (s != MARKER) {
-                    const int dz = z - (int)vz(s);
-                    const int dd = d * d + dz * dz;
-                    if (dd < bestd) { bestd = dd; best = s; }
-                }
+        uint32_t best = line[y];
+        int bestd = best != MARKER ? (z - (int)vz(best)) * (z - (int)vz(best)) : 0x7fffffff;
+        // PBA_U distances per iteration (2 PBA_U loads in flight); the visiting
+        // order (y - d before y + d, d ascending) and the strict improvement
+        // rule are those of a one-step search, so ties resolve the same way
+        for (int d = 1; d * d < bestd; d += PBA_U) {
+            if (y - d < 0 && y + d >= G) break;
+            uint32_t c[2 * PBA_U];
+#pragma unroll
+            for (int q = 0; q < PBA_U; ++q) {
+                c[2 * q] = y - d - q >= 0 ? line[y - d - q] : MARKER;
+                c[2 * q + 1] = y + d + q < G ? line[y + d + q] : MARKER;
             }
-            if (d > 0 && yb < G) {
-                const uint32_t s = line[yb];
-                if (s != MARKER) {
-                    const int dz = z - (int)vz(s);
-                    const int dd = d * d + dz * dz;
-                    if (dd < bestd) { bestd = dd; best = s; }
-                }
+#pragma unroll
+            for (int q = 0; q < 2 * PBA_U; ++q) {
+                if (c[q] == MARKER) continue;
+                const int dy = d + (q >> 1), dz = z - (int)vz(c[q]);
+                const int dd = dy * dy + dz * dz;
+                if (dd < bestd) { bestd = dd; best = c[q]; }
             }
         }
         res[y * (TX + 1) + xx] = best;
@@ -121,27 +123,26 @@ __global__ void __launch_bounds__(256) k_pba_x(int G, const uint32_t* __restrict
         const int row = k / G, x = k % G;
         const int y = y0 + row;
         const uint32_t* line = tile + row * G;
-        uint32_t best = MARKER;
+        uint32_t best = line[x];
         int bestd = 0x7fffffff;
-        for (int d = 0;; ++d) {
-            if (d * d >= bestd) break;
-            const int xa = x - d, xb = x + d;
-            if (xa < 0 && xb >= G) break;
-            if (xa >= 0) {
-                const uint32_t s = line[xa];
-                if (s != MARKER) {
-                    const int dy = y - (int)vy(s), dz = z - (int)vz(s);
-                    const int dd = d * d + dy * dy + dz * dz;
-                    if (dd < bestd) { bestd = dd; best = s; }
-                }
+        if (best != MARKER) {
+            const int dy = y - (int)vy(best), dz = z - (int)vz(best);
+            bestd = dy * dy + dz * dz;
+        }
+        for (int d = 1; d * d < bestd; d += PBA_U) {  // as in the y pass
+            if (x - d < 0 && x + d >= G) break;
+            uint32_t c[2 * PBA_U];
+#pragma unroll
+            for (int q = 0; q < PBA_U; ++q) {
+                c[2 * q] = x - d - q >= 0 ? line[x - d - q] : MARKER;
+                c[2 * q + 1] = x + d + q < G ? line[x + d + q] : MARKER;
             }
-            if (d > 0 && xb < G) {
-                const uint32_t s = line[xb];
-                if (s != MARKER) {
-                    const int dy = y - (int)vy(s), dz = z - (int)vz(s);
-                    const int dd = d * d + dy * dy + dz * dz;
-                    if (dd < bestd) { bestd = dd; best = s; }
-                }
+#pragma unroll
+            for (int q = 0; q < 2 * PBA_U; ++q) {
+                if (c[q] == MARKER) continue;
+                const int dx = d + (q >> 1), dy = y - (int)vy(c[q]), dz = z - (int)vz(c[q]);
+                const int dd = dx * dx + dy * dy + dz * dz;
+                if (dd < bestd) { bestd = dd; best = c[q]; }
             }
         }
         out[base + k] = best;
@@ -276,8 +277,8 @@ void launch_pba_z_stack(const Launch& L, int G, int K, const unsigned long long*
 void launch_pba_y(const Launch& L, int G, const uint32_t* in, uint32_t* out) { launch_pba_y_stack(L, G, 1, in, out); }
 
 void launch_pba_y_stack(const Launch& L, int G, int K, const uint32_t* in, uint32_t* out) {
-    // two tiles of TX*G voxels: 64 KB for G >= 256
-    const int TX = G >= 1024 ? 8 : (G >= 512 ? 16 : 32);
+    // two tiles of TX*G voxels: about 34 KB for G >= 256
+    const int TX = G >= 512 ? 8 : (G >= 256 ? 16 : 32);
     const size_t sm = ((size_t)TX * (G + 1) + (size_t)G * (TX + 1)) * 4;
     switch (TX) {
 #define G4D_Y(T)                                                                                  \
