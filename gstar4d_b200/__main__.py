@@ -1,0 +1,205 @@
+"""Command line with the reference's flags (GDelaunay/Main/Main.cpp:40-207,
+Application.cpp:213-603):
+
+    python -m gstar4d_b200 [-n PointNum] [-g GridSize] [-s Seed] [-r RunNum]
+                           [-d Distribution] [-f FacetMax] [-verbose] [-stats]
+                           [-timing] [-check] [-inFile F] [-outFile F]
+                           [-predThreadNum N] [-predBlockNum N] [-sort]
+                           [-proposal WEIGHTS.npy] [-device D]
+
+Generated points lie in grid units [1, G-2] like the reference's makePoints
+(Application.cpp:316-360) and go through the gdelInit/gdelCompute facade in
+the Morton index space; points read with -inFile (whitespace-separated
+coordinates, duplicates dropped, Application.cpp:475-587) are scaled like
+_scalePoint (Application.cpp:589-603). The generators follow the reference's
+five distributions with this package's own seeded random numbers, so the
+point sets differ from the reference binary's for the same seed.
+-f, -predThreadNum and -predBlockNum are accepted and have no effect (no
+per-loop facet bound, no fixed exact-predicate thread pool). -proposal loads
+learned star-proposal weights (float32[9473], see Triangulator.train_proposal).
+"""
+import sys
+import time
+
+import numpy as np
+
+DISTRIBUTIONS = ("Uniform", "Gaussian", "Ball", "Sphere", "Grid")
+
+USAGE = ("Syntax: gstar4d [-n PointNum] [-g GridSize] [-s Seed] [-r Max] [-d Distribution] [-f FacetMax] "
+         "[-verbose] [-stats] [-timing] [-check] [-inFile F] [-outFile F] [-proposal W.npy] [-device D]\n"
+         "Distribution: 0 - Uniform, 1 - Gaussian, 2 - Ball, 3 - Sphere, 4 - Grid")
+
+
+def parse_args(argv):
+    """Returns the option dict, or raises ValueError on a bad argument."""
+    o = {"seed": 0, "run_num": 1, "grid": 256, "n": 100000, "dist": 0, "facet_max": -1, "verbose": False,
+         "stats": False, "timing": False, "check": False, "in_file": None, "out_file": None,
+         "pred_thread_num": -1, "pred_block_num": -1, "sort": True, "proposal": None, "device": 0, "help": False}
+    valued = {"-n": ("n", int), "-g": ("grid", int), "-r": ("run_num", int), "-s": ("seed", int),
+              "-f": ("facet_max", int), "-d": ("dist", int), "-inFile": ("in_file", str),
+              "-outFile": ("out_file", str), "-predThreadNum": ("pred_thread_num", int),
+              "-predBlockNum": ("pred_block_num", int), "-proposal": ("proposal", str), "-device": ("device", int)}
+    flags = {"-verbose": "verbose", "-stats": "stats", "-timing": "timing", "-check": "check", "-sort": "sort"}
+    i = 0
+    while i < len(argv):
+        a = argv[i]
+        if a in valued:
+            if i + 1 >= len(argv):
+                raise ValueError("missing value for " + a)
+            key, conv = valued[a]
+            o[key] = conv(argv[i + 1])
+            i += 2
+            continue
+        if a in flags:
+            o[flags[a]] = True
+        elif a in ("-h", "--help"):
+            o["help"] = True
+        else:
+            raise ValueError("Error in input argument: " + a)
+        i += 1
+    if not 0 <= o["dist"] < len(DISTRIBUTIONS):
+        raise ValueError("distribution must be 0..4")
+    if o["facet_max"] == -1:  # Main.cpp: 12M for uniform, else 10M (no effect here)
+        o["facet_max"] = 12000000 if o["dist"] == 0 else 10000000
+    return o
+
+
+def make_points(n, grid, dist, seed):
+    """n distinct points in grid units [1, G-2] for the five distributions."""
+    rng = np.random.default_rng(seed)
+    lo, hi = 1.0, float(grid - 2)
+    mid, half = (lo + hi) / 2.0, (hi - lo) / 2.0
+    out, have = [], 0
+    while have < n:
+        m = max(2 * (n - have), 1024)
+        if dist == 0:      # uniform in the cube
+            p = lo + (hi - lo) * rng.random((m, 3))
+        elif dist == 1:    # Gaussian about the centre, kept inside the cube
+            p = rng.normal(mid, half / 6.0, (m, 3))
+            p = p[np.all((p >= lo) & (p <= hi), axis=1)]
+        elif dist == 2:    # uniform in the ball
+            d = rng.normal(size=(m, 3))
+            d /= np.linalg.norm(d, axis=1)[:, None]
+            p = mid + half * d * np.cbrt(rng.random(m))[:, None]
+        elif dist == 3:    # on the sphere
+            d = rng.normal(size=(m, 3))
+            d /= np.linalg.norm(d, axis=1)[:, None]
+            p = mid + half * d
+        else:              # integer grid positions
+            p = np.floor(lo + (hi - lo + 1) * rng.random((m, 3)))
+            p = np.minimum(p, hi)
+        out.append(p)
+        allp = np.concatenate(out)
+        _, first = np.unique(allp, axis=0, return_index=True)
+        out = [allp[np.sort(first)]]
+        have = len(out[0])
+    return np.ascontiguousarray(out[0][:n])
+
+
+def read_points(path):
+    """Whitespace-separated coordinates, three per point, duplicates dropped
+    (first occurrence kept)."""
+    with open(path) as f:
+        vals = np.array(f.read().split(), dtype=np.float64)
+    pts = vals[: len(vals) // 3 * 3].reshape(-1, 3)
+    _, first = np.unique(pts, axis=0, return_index=True)
+    return np.ascontiguousarray(pts[np.sort(first)])
+
+
+def write_ply(path, points, tets):
+    """The reference's TetraMesh::writeToFile layout (Geometry.cu:396-460):
+    ASCII PLY, the vertices, then three faces per tetrahedron."""
+    v = np.asarray(tets["v"] if getattr(tets, "dtype", None) is not None and tets.dtype.names else tets)[:, :4]
+    faces = np.concatenate([v[:, [0, 1, 2]], v[:, [0, 1, 3]], v[:, [0, 2, 3]]], axis=0) if len(v) else np.zeros(
+        (0, 3), np.int64)
+    with open(path, "w") as f:
+        f.write("ply\nformat ascii 1.0\nelement vertex %d\nproperty float x\nproperty float y\nproperty float z\n"
+                "element face %d\nproperty list uchar int vertex_index\nend_header\n" % (len(points), len(faces)))
+        np.savetxt(f, points, fmt="%.9g")
+        np.savetxt(f, np.concatenate([np.full((len(faces), 1), 3), faces], axis=1), fmt="%d")
+
+
+def check_adjacency(tets):
+    """Host check of the output: every neighbour link is reciprocated across the
+    same face. Returns the number of broken links."""
+    v = tets["v"].astype(np.int64)
+    opp = tets["opp"].astype(np.int64)
+    bad = 0
+    faces = {}
+    for t in range(len(v)):
+        for i in range(4):
+            key = tuple(sorted(np.delete(v[t], i)))
+            faces.setdefault(key, []).append((t, i))
+    for t in range(len(v)):
+        for i in range(4):
+            n = opp[t, i]
+            key = tuple(sorted(np.delete(v[t], i)))
+            mates = [u for u, _ in faces[key] if u != t]
+            if n < 0:
+                bad += len(mates) != 0
+            else:
+                bad += mates != [n]
+    return bad
+
+
+def main(argv=None):
+    try:
+        o = parse_args(sys.argv[1:] if argv is None else argv)
+    except ValueError as e:
+        print(str(e) + "\n\n" + USAGE)
+        return 1
+    if o["help"]:
+        print(USAGE)
+        return 1
+    import gstar4d_b200
+    print("GDelaunay ... Seed: %d RunNum: %d Dist: %d Grid: %d %s" % (
+        o["seed"], o["run_num"], o["dist"], o["grid"],
+        ("Input: " + o["in_file"]) if o["in_file"] else ("Points: %d" % o["n"])))
+    weights = np.load(o["proposal"]).astype(np.float32) if o["proposal"] else None
+    cfg = dict(grid_size=o["grid"], do_check=int(o["check"]), log_verbose=int(o["verbose"]),
+               log_stats=int(o["stats"]), log_timing=int(o["timing"]), device=o["device"],
+               facet_max=o["facet_max"], pred_thread_num=o["pred_thread_num"],
+               pred_block_num=o["pred_block_num"], proposal=int(weights is not None))
+    totals = []
+    for run in range(o["run_num"]):
+        with gstar4d_b200.Triangulator(**cfg) as t:
+            if weights is not None:
+                t.proposal_weights(weights)
+            t0 = time.perf_counter()
+            if o["in_file"]:
+                pts = read_points(o["in_file"])
+                tets, _, st = t.triangulate(pts)
+                times = (st["t_pba_ms"], st["t_star_ms"], st["t_splay_ms"], st["t_out_ms"])
+            else:
+                pts = make_points(o["n"], o["grid"], o["dist"], o["seed"] + run)
+                work = pts.copy()
+                t.gdel_init(work)
+                times = t.gdel_compute()
+                tets = t.get_tetra_from_gpu()
+                st = t.stats()
+                t.gdel_deinit()
+                pts = work  # the tetrahedra index the Morton-sorted points
+            wall = (time.perf_counter() - t0) * 1e3
+        total = sum(times)
+        totals.append(total)
+        if o["timing"] or o["verbose"]:
+            print("PBA: %.3f ms  InitStar: %.3f ms  Consistent: %.3f ms  Output: %.3f ms" % tuple(times))
+        if o["stats"] or o["verbose"]:
+            print("Star insertions: %d  Splay insertions: %d  Loops: %d  Tetra: %d  Exact predicates: %d" % (
+                st["star_insertions"], st["splay_insertions"], st["loops"], len(tets), st["exact_predicates"]))
+        print("Total Time: %.3f ms (call %.3f ms)" % (total, wall))
+        if o["check"]:
+            bad = check_adjacency(tets)
+            print("Check: stars consistent on the device; %s" % (
+                "adjacency OK" if bad == 0 else "%d adjacency links broken" % bad))
+            if bad:
+                return 2
+        if o["out_file"]:
+            write_ply(o["out_file"], pts, tets)
+    if o["run_num"] > 1:
+        print("Average Total Time: %.3f ms" % (sum(totals) / len(totals)))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

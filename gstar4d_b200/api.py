@@ -60,7 +60,7 @@ _lib = None
 
 EXPORTS = ["g4d_default_config", "g4d_create", "g4d_destroy", "g4d_last_error", "g4d_status_string",
            "g4d_triangulate", "g4d_triangulate_to", "g4d_triangulate_device", "g4d_gdel_init",
-           "g4d_gdel_compute", "g4d_get_tetra", "g4d_gdel_deinit", "g4d_triangulate_batch",
+           "g4d_gdel_compute", "g4d_get_tetra", "g4d_gdel_deinit", "g4d_get_stats", "g4d_triangulate_batch",
            "g4d_triangulate_batch_device", "g4d_stream",
            "g4d_eval_predicates", "g4d_voronoi", "g4d_voronoi_noalloc", "g4d_proposal_train",
            "g4d_proposal_weights", "g4d_mlp_grad", "g4d_mlp_infer", "g4d_free"]
@@ -91,6 +91,7 @@ def load():
     L.g4d_gdel_compute.argtypes = [vp, dp, dp, dp, dp]
     L.g4d_get_tetra.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(ip)]
     L.g4d_gdel_deinit.argtypes = [vp]
+    L.g4d_get_stats.argtypes = [vp, ctypes.POINTER(Stats)]
     L.g4d_triangulate_batch.argtypes = [vp, vp, vp, ip, ctypes.POINTER(vp), ctypes.POINTER(vp),
                                         ctypes.POINTER(Stats)]
     L.g4d_triangulate_batch_device.argtypes = [vp, vp, vp, ip, ctypes.POINTER(vp), ctypes.POINTER(vp),
@@ -278,6 +279,12 @@ class Triangulator:
             return np.empty(0, TET_DTYPE)
         buf = (ctypes.c_char * (nt.value * TET_DTYPE.itemsize)).from_address(p.value)
         return np.frombuffer(buf, TET_DTYPE).copy()
+
+    def stats(self):
+        """Statistics of the last triangulation on this context."""
+        st = Stats()
+        self._check(self._lib.g4d_get_stats(self._h, ctypes.byref(st)))
+        return st.as_dict()
 
     def gdel_deinit(self):
         self._check(self._lib.g4d_gdel_deinit(self._h))

@@ -1200,6 +1200,12 @@ g4d_status g4d_get_tetra(g4d_ctx* ctx, const g4d_tet** tets, int* ntet) {
     return G4D_OK;
 }
 
+g4d_status g4d_get_stats(const g4d_ctx* ctx, g4d_stats* stats) {
+    if (!ctx || !stats) return G4D_ERR_ARG;
+    *stats = ctx->stats;
+    return G4D_OK;
+}
+
 g4d_status g4d_gdel_deinit(g4d_ctx* ctx) {
     if (!ctx) return G4D_ERR_ARG;
     ctx->gdel_ready = false;

@@ -133,6 +133,9 @@ G4D_API g4d_status g4d_gdel_compute(g4d_ctx* ctx, double* t_pba, double* t_star,
  * next compute or deinit. */
 G4D_API g4d_status g4d_get_tetra(g4d_ctx* ctx, const g4d_tet** tets, int* ntet);
 G4D_API g4d_status g4d_gdel_deinit(g4d_ctx* ctx);
+/* Statistics of the context's last triangulation (the counters the reference
+ * prints with -stats / -timing, GDelHost.cu:101-113). */
+G4D_API g4d_status g4d_get_stats(const g4d_ctx* ctx, g4d_stats* stats);
 
 /* Batched triangulation of many clouds. The reference is one cloud per process
  * with global state (GDelHost.cu:57-113), so this has no counterpart there; each
