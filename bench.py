@@ -50,6 +50,19 @@ METRIC = "Mpts/s to bit-exact 3D DT on 1 B200"
 SAMPLE_POINTS, SAMPLE_GRID = 125_000, 256  # same voxel density (134 voxels/point)
 
 
+def _pba_traffic(G):
+    """DRAM bytes of one PBA (z, y, x passes) from the committed ncu summary,
+    scaled from its grid to G by the voxel count; None when absent."""
+    try:
+        with open(os.path.join(REPO, "profiles", "pba_mixed100k_g512.md")) as f:
+            for line in f:
+                if line.startswith("traffic_per_launch_bytes:"):
+                    return float(line.split()[1]) * (G / 512.0) ** 3
+    except OSError:
+        pass
+    return None
+
+
 def _peaks():
     try:
         with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
@@ -402,7 +415,8 @@ def main():
                     "d2h_bytes_per_step": int(len(tets) * 32)},
             "roofline": {"kernel": "pba (z,y,x passes)", "bound": "hbm", "achieved": round(achieved, 1),
                          "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                         "traffic": None, "algorithmic_bytes": alg_bytes, "avg_ms": round(pba_avg, 4)},
+                         "traffic": _pba_traffic(G), "traffic_source": "profiles/pba_mixed100k_g512.md (ncu)",
+                         "algorithmic_bytes": alg_bytes, "avg_ms": round(pba_avg, 4)},
             "stages_ms": {k: round(last[k], 3) for k in ("t_init_ms", "t_pba_ms", "t_star_ms", "t_splay_ms",
                                                           "t_out_ms", "t_total_ms")},
             "splay": {"loops": last["loops"], "star_insertions_per_point": round(last["star_insertions"] / n, 3),

@@ -38,12 +38,12 @@ __global__ void __launch_bounds__(128) k_pba_z(int G, const KeyT* __restrict__ c
     int i = cs[c];
     const int e = ce[c];
     uint32_t* o = out + (size_t)blockIdx.z * plane * G + (size_t)y * G + x;
-    if (i >= e) {
-        for (int z = 0; z < G; ++z) o[z * plane] = MARKER;
-        return;
-    }
+    // empty columns run the same loop so that the warp stays together: each
+    // store is then one full 128-byte line (a store split by divergence
+    // writes partial sectors, which L2 fills from DRAM first)
+    const bool empty = i >= e;
     int prev = -(1 << 20);
-    int next = (int)(ckey[i] & 1023u);
+    int next = empty ? (1 << 20) : (int)(ckey[i] & 1023u);
     for (int z = 0; z < G; ++z) {
         while (next <= z) {
             prev = next;
@@ -51,7 +51,9 @@ __global__ void __launch_bounds__(128) k_pba_z(int G, const KeyT* __restrict__ c
             next = i < e ? (int)(ckey[i] & 1023u) : (1 << 20);
         }
         const int zs = (z - prev <= next - z) ? prev : next;
-        o[z * plane] = enc_vox(x, y, zs);
+        const uint32_t v = empty ? MARKER : enc_vox(x, y, zs);
+        __syncwarp();
+        o[z * plane] = v;
     }
 }
 
