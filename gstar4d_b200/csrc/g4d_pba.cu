@@ -174,13 +174,31 @@ __device__ __forceinline__ void pair_hash_insert(unsigned long long* hs, unsigne
 // Candidate Delaunay edges: every two distinct sites of a 2x2x2 voxel cube in
 // which at least four sites meet (a digital Voronoi vertex: its sites are
 // pairwise Voronoi neighbours; the reference reads the same cubes and emits
-// around digital Voronoi vertices, GDelKernels.cu:137-299). One thread sweeps a column of cubes along z,
-// keeping the previous voxel plane in registers (4 new loads per cube,
-// coalesced over x); a per-thread cache of the last pairs and a block-local
-// hash remove duplicates before the per-star scatter.
+// around digital Voronoi vertices, GDelKernels.cu:137-299). One thread sweeps a
+// column of cubes along z, keeping the previous voxel plane in registers (4 new
+// loads per cube, coalesced over x). Vertex cubes are rare: a lane queues the
+// site set of each one (skipping a repeat of its previous set) in a per-warp
+// queue, and every 32 queued cubes the warp emits their pairs, one cube per
+// lane, into a block-local hash that removes duplicates before the per-star
+// scatter.
+// all pairs of one queued vertex cube into the block hash
+template <class KeyT>
+__device__ __forceinline__ void emit_cube(unsigned long long* hs, const uint32_t* q, int ns, const Dev& D,
+                                          const Cols<KeyT>& C) {
+    for (int i = 0; i < ns; ++i)
+        for (int j = i + 1; j < ns; ++j) {
+            const uint32_t lo = q[i] < q[j] ? q[i] : q[j], hi = q[i] < q[j] ? q[j] : q[i];
+            pair_hash_insert(hs, ((unsigned long long)lo << 32) | hi, D, C);
+        }
+}
+
+constexpr int PAIR_QUEUE = 64;  // queued vertex cubes per warp
+
 template <class KeyT>
 __global__ void __launch_bounds__(128) k_pairs(Dev D, const uint32_t* __restrict__ stack, Cols<KeyT> C, int nzc) {
     __shared__ unsigned long long hs[PAIR_HASH];
+    __shared__ uint32_t qs[4][PAIR_QUEUE][8];  // site sets of vertex cubes
+    __shared__ uint8_t qn[4][PAIR_QUEUE];
     const int G = C.G;
     const int tid = threadIdx.y * 32 + threadIdx.x;
     for (int k = tid; k < PAIR_HASH; k += 128) hs[k] = ~0ull;
@@ -193,7 +211,7 @@ __global__ void __launch_bounds__(128) k_pairs(Dev D, const uint32_t* __restrict
     const uint32_t* grid = stack + (size_t)kk * plane * G;
     C.start += (size_t)kk * plane;
     C.end += (size_t)kk * plane;
-    const int lane = threadIdx.x;
+    const int lane = threadIdx.x, w = threadIdx.y;
     // every lane of the warp walks the same z range so the warp collectives
     // below stay converged; lanes past the grid edge carry no pairs
     const bool active = x < G - 1 && y < G - 1;
@@ -202,40 +220,56 @@ __global__ void __launch_bounds__(128) k_pairs(Dev D, const uint32_t* __restrict
         const uint32_t* g = grid + (size_t)y * G + (active ? x : 0);
         uint32_t a0 = g[(size_t)z0 * plane], a1 = g[(size_t)z0 * plane + 1];
         uint32_t a2 = g[(size_t)z0 * plane + G], a3 = g[(size_t)z0 * plane + G + 1];
-        unsigned long long recent[4] = {~0ull, ~0ull, ~0ull, ~0ull};
-        int rp = 0;
+        unsigned long long last = 0;  // signature of the set this lane queued last
+        int qc = 0;                   // queued cubes of this warp (same in every lane)
         for (int z = z0; z < zend; ++z) {
             const size_t o = (size_t)(z + 1) * plane;
             const uint32_t b0 = g[o], b1 = g[o + 1], b2 = g[o + G], b3 = g[o + G + 1];
-            const uint32_t v[8] = {a0, a1, a2, a3, b0, b1, b2, b3};
-            uint32_t s[8];
+            bool cand = false;
+            uint32_t sset[8];
             int ns = 0;
+            // most cubes lie inside one Voronoi cell: four sites need at least
+            // three voxels that differ from a0
+            const int diff = (a1 != a0) + (a2 != a0) + (a3 != a0) + (b0 != a0) + (b1 != a0) + (b2 != a0) + (b3 != a0);
+            if (active && diff >= 3) {
+                const uint32_t v[8] = {a0, a1, a2, a3, b0, b1, b2, b3};
 #pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                bool dup = false;
-                for (int k = 0; k < ns; ++k) dup |= (s[k] == v[i]);
-                if (!dup) s[ns++] = v[i];
-            }
-            const int np = (active && ns >= 4) ? ns * (ns - 1) / 2 : 0;
-            const int maxp = __reduce_max_sync(0xffffffffu, (unsigned)np);
-            int pi = 0, pj = 1;
-            for (int k = 0; k < maxp; ++k) {
-                unsigned long long key = ~0ull;
-                if (k < np) {
-                    const uint32_t lo = s[pi] < s[pj] ? s[pi] : s[pj], hi = s[pi] < s[pj] ? s[pj] : s[pi];
-                    key = ((unsigned long long)lo << 32) | hi;
-                    if (++pj == ns) { ++pi; pj = pi + 1; }
-                    if (key == recent[0] || key == recent[1] || key == recent[2] || key == recent[3])
-                        key = ~0ull;
-                    else
-                        recent[(rp++) & 3] = key;
+                for (int i = 0; i < 8; ++i) {
+                    bool dup = false;
+                    for (int k = 0; k < ns; ++k) dup |= (sset[k] == v[i]);
+                    if (!dup) sset[ns++] = v[i];
                 }
-                // lanes holding the same pair elect one inserter
-                const unsigned grp = __match_any_sync(0xffffffffu, key);
-                if (key != ~0ull && lane == __ffs(grp) - 1) pair_hash_insert(hs, key, D, C);
+                if (ns >= 4) {
+                    // consecutive cubes around one Voronoi vertex repeat its set
+                    unsigned long long sum = 0, xr = 0;
+                    for (int k = 0; k < ns; ++k) { sum += sset[k]; xr ^= (unsigned long long)sset[k] * 0x9E3779B97F4A7C15ull; }
+                    const unsigned long long sig = (sum << 32) ^ xr ^ (unsigned long long)ns;
+                    cand = sig != last;
+                    last = sig;
+                }
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, cand);
+            if (cand) {
+                const int pos = qc + __popc(m & ((1u << lane) - 1u));
+                for (int k = 0; k < ns; ++k) qs[w][pos][k] = sset[k];
+                qn[w][pos] = (uint8_t)ns;
+            }
+            qc += __popc(m);
+            if (qc >= 32) {  // one queued cube per lane
+                __syncwarp();
+                emit_cube(hs, qs[w][lane], qn[w][lane], D, C);
+                __syncwarp();
+                for (int k = 32 + lane; k < qc; k += 32) {
+                    for (int q = 0; q < qn[w][k]; ++q) qs[w][k - 32][q] = qs[w][k][q];
+                    qn[w][k - 32] = qn[w][k];
+                }
+                qc -= 32;
+                __syncwarp();
             }
             a0 = b0; a1 = b1; a2 = b2; a3 = b3;
         }
+        __syncwarp();
+        if (lane < qc) emit_cube(hs, qs[w][lane], qn[w][lane], D, C);
     }
     __syncthreads();
     for (int k = tid; k < PAIR_HASH; k += 128) {
