@@ -52,7 +52,7 @@ enum BufId {
     B_XYZ, B_GRIDSRC, B_MM, B_KEYS, B_VALS, B_VOXIN, B_MKEY, B_ORDER, B_P, B_VOX, B_CKEY0, B_CID0, B_CKEY,
     B_CID, B_COLS, B_COLE, B_GA, B_GB, B_BUCKET, B_BCOUNT, B_HH, B_TRI, B_HDR, B_INBOX, B_ICOUNT, B_WLINS,
     B_WLEMIT, B_WLEMIT2, B_DROWN, B_DROWN2, B_CTR, B_CNT, B_BASE, B_TETS, B_CUB, B_BAD, B_LIDX, B_LHH, B_LTRI,
-    B_WLINSL, B_WLPROM, B_SKEY0, B_SKEY, B_GIDX, B_LOCAL, B_BCKEY0, B_BCKEY, B_SLOTS, B_MMB, B_TC, B_TETS2, B_OVF, B_OVF2, B_KMASK, B_BOUT, B_OCC,
+    B_WLINSL, B_WLPROM, B_SKEY0, B_SKEY, B_GIDX, B_LOCAL, B_BCKEY0, B_BCKEY, B_SLOTS, B_MMB, B_TC, B_TETS2, B_OVF, B_OVF2, B_KMASK, B_BOUT, B_OCC, B_WLEXACT, B_WLBIG,
     B_MLP_P, B_MLP_G, B_MLP_M1, B_MLP_M2, B_MLP_AUX, B_RING_PAIR, B_RING_X, B_RING_Y, B_RING_LOGIT, B_TILES,
     B_DIAG_X, B_DIAG_Y, B_DIAG_P, B_DIAG_G, B_NUM
 };
@@ -146,6 +146,8 @@ Dev make_dev(g4d_ctx* ctx) {
     D.largeCap = ctx->large_cap;
     D.wlInsL = ctx->b[B_WLINSL].as<int>();
     D.wlPromote = ctx->b[B_WLPROM].as<int>();
+    D.wlExact = ctx->b[B_WLEXACT].as<int>();
+    D.wlBig = ctx->b[B_WLBIG].as<int>();
     D.anyLarge = 0;
     D.keptMask = ctx->b[B_KMASK].as<uint32_t>();
     D.ovf = ctx->b[B_OVF].as<int2>();
@@ -290,6 +292,8 @@ g4d_status alloc_stars(g4d_ctx* ctx, int n) {
     CK(ctx->b[B_BAD].ensure(64));
     CK(ctx->b[B_LIDX].ensure(sizeof(int) * n));
     CK(ctx->b[B_WLPROM].ensure(sizeof(int) * n));
+    CK(ctx->b[B_WLEXACT].ensure(sizeof(int) * n));
+    CK(ctx->b[B_WLBIG].ensure(sizeof(int) * n));
     CK(ctx->b[B_OVF].ensure(sizeof(int2) * (8 * (size_t)n + 1024)));
     CK(ctx->b[B_OVF2].ensure(sizeof(int2) * (8 * (size_t)n + 1024)));
     CK(ctx->b[B_KMASK].ensure(sizeof(uint32_t) * (TSTRIDE / 32) * (size_t)n));
@@ -341,15 +345,31 @@ g4d_status run_splay(g4d_ctx* ctx, Dev& D) {
     CK(cudaMemsetAsync(ctx->b[B_ICOUNT].p, 0, sizeof(int) * n, ctx->stream));
     CK(cudaMemsetAsync(ctx->b[B_INBOX].p, 0xff, sizeof(int) * (size_t)n * INBOX_CAP, ctx->stream));
     CK(cudaMemsetAsync(ctx->b[B_LIDX].p, 0xff, sizeof(int) * n, ctx->stream));
-    launch_star_build(L, D);
-    cudaEventRecord(ctx->ev[3], ctx->stream);
-
     Counters h{};
     Counters* dctr = D.ctr;
-    CK(cudaMemcpyAsync(&h, dctr, sizeof(Counters), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-    g4d_status st = check_err(ctx, h.err);
+    auto read = [&]() -> g4d_status {
+        CK(cudaMemcpyAsync(&h, dctr, sizeof(Counters), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        return check_err(ctx, h.err);
+    };
+    // initial stars: filter-only, then the exact kernel for the stars it left,
+    // then the large class for stars too big for the small one
+    launch_star_build(L, D, nullptr, n, false);
+    g4d_status st = read();
     if (st) return st;
+    if (h.exact_next) {
+        launch_star_build(L, D, D.wlExact, h.exact_next, true);
+        if ((st = read())) return st;
+    }
+    if (h.build_big) {
+        st = grow_large(ctx, D, h.large_next, h.large_next + h.build_big);
+        if (st) return st;
+        D.anyLarge = 1;
+        launch_star_build_large(L, D, D.wlBig, h.build_big);
+        if ((st = read())) return st;
+    }
+    cudaEventRecord(ctx->ev[3], ctx->stream);
+    CK(cudaMemsetAsync(&dctr->exact_next, 0, 2 * sizeof(int), ctx->stream));  // exact_next, build_big
     const unsigned long long built = h.insertions;  // initial workset insertions
     int emitCount = h.emit_next, drownCount = h.drown_next, ovfCount = h.ovf_next;
     // the lists produced by the build become the current ones
@@ -382,12 +402,13 @@ g4d_status run_splay(g4d_ctx* ctx, Dev& D) {
         if (st) return st;
         if (h.ins_count == 0 && h.ins_count_large == 0) break;
         ovfCount = h.ovf_next;  // requests that found a full inbox this round
-        if (h.ins_count) launch_star_insert(L, D, h.ins_count);
+        if (h.ins_count) launch_star_insert(L, D, D.wlIns, h.ins_count, false);
         if (h.ins_count_large) launch_star_insert_large(L, D, D.wlInsL, std::min(h.ins_count_large, D.largeCap));
-        CK(cudaMemcpyAsync(&h, dctr, sizeof(Counters), cudaMemcpyDeviceToHost, ctx->stream));
-        CK(cudaStreamSynchronize(ctx->stream));
-        st = check_err(ctx, h.err);
-        if (st) return st;
+        if ((st = read())) return st;
+        if (h.exact_next) {  // stars the filter-only kernel could not decide
+            launch_star_insert(L, D, D.wlExact, h.exact_next, true);
+            if ((st = read())) return st;
+        }
         if (h.promote_count) {
             // stars that outgrew the small class: move them, then replay their round
             st = grow_large(ctx, D, h.large_next, h.large_next + h.promote_count);
@@ -405,8 +426,8 @@ g4d_status run_splay(g4d_ctx* ctx, Dev& D) {
         std::swap(D.wlEmit, D.wlEmitNext);
         std::swap(D.drown, D.drownNext);
         std::swap(D.ovf, D.ovfNext);
-        // ins_count, emit_next, drown_next, ins_count_large, promote_count
-        CK(cudaMemsetAsync(dctr, 0, 5 * sizeof(int), ctx->stream));
+        // ins_count, emit_next, drown_next, ins_count_large, promote_count, exact_next, build_big
+        CK(cudaMemsetAsync(dctr, 0, 7 * sizeof(int), ctx->stream));
         CK(cudaMemsetAsync(&dctr->ovf_next, 0, sizeof(int), ctx->stream));
     }
     cudaEventRecord(ctx->ev[4], ctx->stream);

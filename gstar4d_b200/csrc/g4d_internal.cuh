@@ -4,9 +4,9 @@
 //   P        double4[n]     points in Morton order (x,y,z,0): one 32-byte sector each
 //   vox      uint32[n]      voxel of each point, packed x | y<<10 | z<<20
 //   grid A/B uint32[G^3]    digital Voronoi sites, packed voxel coords, x fastest
-//   hh       int32[n*512]   per-star history hash: every point ever inserted in the
+//   hh       int32[n*256]   per-star history hash: every point ever inserted in the
 //                           star (bit 31 = currently in the link), open addressing
-//   tri      uint2[n*224]   per-star link triangles, 8 bytes each (packing below)
+//   tri      uint2[n*128]   per-star link triangles, 8 bytes each (packing below)
 //   lhh/ltri                the same for the few stars promoted to the large class
 //                           (4096 hash slots, 2048 triangles of 16 bytes)
 //   hdr      StarHdr[n]     triangle count, history count, pass number, flags
@@ -38,10 +38,10 @@ constexpr uint32_t MARKER = 0xffffffffu;  // voxel without a site
 // Two star storage classes. Every star starts in the small class; a star whose
 // history or link outgrows it (points next to a dense sheet of points, e.g. a
 // sampled sphere) moves to the large class between kernels.
-constexpr int HSLOTS = 512;               // small: history hash slots per star
-constexpr int HMAX = 255;                 // small: max history entries (hash load <= 1/2)
-constexpr int TMAX = 220;                 // small: max link triangles (a link of 112 points)
-constexpr int TSTRIDE = 224;              // small: triangle slots per star in HBM
+constexpr int HSLOTS = 256;               // small: history hash slots per star
+constexpr int HMAX = 127;                 // small: max history entries (hash load <= 1/2)
+constexpr int TMAX = 124;                 // small: max link triangles (a link of 64 points)
+constexpr int TSTRIDE = 128;              // small: triangle slots per star in HBM
 constexpr int LHSLOTS = 4096;             // large: history hash slots
 constexpr int LHMAX = 2047;               // large: max history entries
 constexpr int LTMAX = 2044;               // large: max link triangles
@@ -79,6 +79,8 @@ struct Counters {
     int drown_next;       // drowned items for next round
     int ins_count_large;  // large stars queued for insertion
     int promote_count;    // small stars that outgrew their class this round
+    int exact_next;       // stars the filter-only kernel left for the exact kernel
+    int build_big;        // initial stars too large for the small class
     int large_next;       // large-class slots handed out so far
     int ovf_next;         // insertion requests that found a full inbox (next round)
     int overflow;         // inbox overflow happened
@@ -153,6 +155,8 @@ struct Dev {
     int largeCap;
     int* wlInsL;           // large stars with inbox requests
     int* wlPromote;        // small stars to move to the large class
+    int* wlExact;          // stars that need the exact-predicate kernel
+    int* wlBig;            // initial stars to build in the large class
     int anyLarge;          // some star is in the large class (else lidx is not read)
     uint32_t* keptMask;    // small stars: kept-triangle bits (TSTRIDE / 32 words each)
     // requests (star, point) that found the star's inbox full: re-sent next round
@@ -245,8 +249,13 @@ void launch_pairs_stack(const Launch& L, const Dev& D, const uint32_t* stack, in
 void launch_missing_u64(const Launch& L, const Dev& D, const unsigned long long* mkey);
 
 // stars
-void launch_star_build(const Launch& L, const Dev& D);
-void launch_star_insert(const Launch& L, const Dev& D, int count);
+// Star kernels run first filter-only (exact = false: FP64 filter, no exact
+// arithmetic in the kernel, more resident warps); a star that meets an
+// undecided predicate is left untouched and listed in wlExact for the same
+// kernel with exact predicates (exact = true).
+void launch_star_build(const Launch& L, const Dev& D, const int* list, int count, bool exact);
+void launch_star_build_large(const Launch& L, const Dev& D, const int* list, int count);
+void launch_star_insert(const Launch& L, const Dev& D, const int* list, int count, bool exact);
 void launch_star_insert_large(const Launch& L, const Dev& D, const int* list, int count);
 void launch_promote(const Launch& L, const Dev& D, int count);
 void launch_requeue(const Launch& L, const Dev& D, int count);

@@ -31,8 +31,9 @@ constexpr int WARPS_PER_BLOCK = 4;
 // ---------------------------------------------------------------------------
 
 struct SmallStar {
-    static constexpr int LOG2_HS = 9, HS = HSLOTS, HM = HMAX, TM = TMAX, TS = TSTRIDE;
-    static constexpr int WARPS = WARPS_PER_BLOCK, MINB = 4;
+    static constexpr int LOG2_HS = 8, HS = HSLOTS, HM = HMAX, TM = TMAX, TS = TSTRIDE;
+    // blocks per SM: 6 filter-only (about 80 registers), 4 with the exact path
+    static constexpr int WARPS = WARPS_PER_BLOCK, MINB = 4, MINB_FAST = 6;
     static constexpr bool LARGE = false;
     using Idx = uint8_t;   // triangle index and coordinate-cache index
     using Rec = uint32_t;  // hole boundary edge: u | w<<9 | o<<18 | oj<<26
@@ -61,7 +62,7 @@ struct SmallStar {
 //   w = o2 | j0<<16 | j1<<18 | j2<<20
 struct LargeStar {
     static constexpr int LOG2_HS = 12, HS = LHSLOTS, HM = LHMAX, TM = LTMAX, TS = LTSTRIDE;
-    static constexpr int WARPS = 1, MINB = 1;  // about 141 KB of shared memory per warp
+    static constexpr int WARPS = 1, MINB = 1, MINB_FAST = 1;  // about 141 KB of shared memory per warp
     static constexpr bool LARGE = true;
     using Idx = uint16_t;
     using Rec = unsigned long long;  // u | w<<12 | o<<24 | oj<<35
@@ -94,7 +95,7 @@ struct LargeStar {
     __device__ static Tri* tris(const Dev& D, int s) { return D.ltri + (size_t)D.lidx[s] * TS; }
 };
 
-// Per-warp shared-memory image of one star (14 KB small, so that 16 warps fit
+// Per-warp shared-memory image of one star (7.4 KB small, so that 24 warps fit
 // on an SM; 141 KB large).
 template <class C>
 struct WS {
@@ -120,7 +121,7 @@ struct WS {
 };
 
 // 4 blocks of 4 warps per SM: 16 images plus the per-block reservation in 228 KB
-static_assert(4 * (4 * sizeof(WS<SmallStar>) + 1024) <= 228 * 1024, "small star image too large");
+static_assert(SmallStar::MINB_FAST * (4 * sizeof(WS<SmallStar>) + 1024) <= 228 * 1024, "small star image too large");
 static_assert(sizeof(WS<LargeStar>) + 1024 <= 227 * 1024, "large star image too large");
 
 // Read-only view of any star, whichever class holds it (cross-star lookups).
@@ -211,6 +212,14 @@ __device__ __forceinline__ PredSink sink_of(const Dev& D) {
     k.dbg_pts = D.ctr->dbg_pts;
     k.dbg_ids = D.ctr->dbg_ids;
     return k;
+}
+
+// lifted orientation: exact (never 0) or the FP64 filter alone (0 = undecided)
+template <bool EXACT>
+__device__ __forceinline__ int pred4(double3 a, double3 b, double3 c, double3 d, double3 e, int ia, int ib, int ic,
+                                     int id, int ie, const PredSink& sink, unsigned* exact) {
+    if (EXACT) return orient4(a, b, c, d, e, ia, ib, ic, id, ie, sink, exact);
+    return orient4_filter(a, b, c, d, e);
 }
 
 // point coordinates; an out-of-range id (only possible from a corrupted star)
@@ -325,8 +334,9 @@ __device__ __forceinline__ int ws_hash_insert(WS<C>& S, int v, bool* fresh) {
 // Insert the point in slot sp into the star held by the warp. Returns 1 when it
 // entered the link, 0 when it lies inside the star's cone (drowned), -1 on an
 // error (flag raised), -2 when the star's class has no room for the new
-// triangles (the caller promotes the star or reports the capacity error).
-template <class C>
+// triangles (the caller promotes the star or reports the capacity error), -3
+// when a filter-only kernel meets an undecided predicate (nothing changed).
+template <class C, bool EXACT>
 __device__ int warp_insert(WS<C>& S, int lane, int s, double3 ps, int sp, int gen, const PredSink& sink,
                            unsigned* exact) {
     using Idx = typename C::Idx;
@@ -335,21 +345,26 @@ __device__ int warp_insert(WS<C>& S, int lane, int s, double3 ps, int sp, int ge
     const int pid = wid(S, sp);
     const int ntri = S.ntri;
     int nb = 0, nalive = 0;
+    bool undecided = false;
     for (int base = 0; base < ntri; base += 32) {
         const int t = base + lane;
-        bool b = false, al = false;
+        bool b = false, al = false, und = false;
         if (t < ntri && (S.tf[t] & 0x80)) {
             al = true;
             const int a = S.tv[0][t], bb = S.tv[1][t], c = S.tv[2][t];
-            b = orient4(wpt(S, a), wpt(S, bb), wpt(S, c), ps, pp, wid(S, a), wid(S, bb), wid(S, c), s, pid, sink,
-                        exact) < 0;
+            const int sg = pred4<EXACT>(wpt(S, a), wpt(S, bb), wpt(S, c), ps, pp, wid(S, a), wid(S, bb), wid(S, c),
+                                        s, pid, sink, exact);
+            b = sg < 0;
+            und = sg == 0;
         }
         const unsigned m = __ballot_sync(0xffffffffu, b);
         nalive += __popc(__ballot_sync(0xffffffffu, al));
+        if (!EXACT) undecided |= __any_sync(0xffffffffu, und);
         if (lane == 0) S.bmask[base >> 5] = m;
         nb += __popc(m);
     }
     __syncwarp();
+    if (!EXACT && undecided) return -3;
     if (nb == 0) return 0;
     if (nb == nalive) {
         if (lane == 0) {
@@ -454,12 +469,14 @@ __device__ int warp_insert(WS<C>& S, int lane, int s, double3 ps, int sp, int ge
 
 // cone of the pentachoron (l0..l3, star): the link triangles of the 4-simplex
 // (GDelPredKernels.cu:45-158), oriented so that orient4(tri, star, opposite) > 0
-template <class C>
-__device__ void warp_cone(WS<C>& S, int lane, int s, double3 ps, const int* l4, int gen, const PredSink& sink,
-                          unsigned* exact) {
+// returns 0, or -3 when a filter-only kernel cannot orient the pentachoron
+template <class C, bool EXACT>
+__device__ int warp_cone(WS<C>& S, int lane, int s, double3 ps, const int* l4, int gen, const PredSink& sink,
+                         unsigned* exact) {
     int l[4] = {l4[0], l4[1], l4[2], l4[3]};
-    const int o = orient4(wpt(S, l[0]), wpt(S, l[1]), wpt(S, l[2]), wpt(S, l[3]), ps, wid(S, l[0]), wid(S, l[1]),
-                          wid(S, l[2]), wid(S, l[3]), s, sink, exact);
+    const int o = pred4<EXACT>(wpt(S, l[0]), wpt(S, l[1]), wpt(S, l[2]), wpt(S, l[3]), ps, wid(S, l[0]),
+                               wid(S, l[1]), wid(S, l[2]), wid(S, l[3]), s, sink, exact);
+    if (!EXACT && o == 0) return -3;
     if (o < 0) { const int t = l[0]; l[0] = l[1]; l[1] = t; }
     if (lane < 4) {
         const int F[4][3] = {{1, 2, 3}, {0, 3, 2}, {0, 1, 3}, {0, 2, 1}};
@@ -480,6 +497,7 @@ __device__ void warp_cone(WS<C>& S, int lane, int s, double3 ps, const int* l4, 
         S.nfree = 0;
     }
     __syncwarp();
+    return 0;
 }
 
 // sort order[0..n) by okey ascending (bitonic over a power of two <= HM + 1)
@@ -607,22 +625,29 @@ __device__ void warp_store(WS<C>& S, const Dev& D, int lane, int s, int pass, bo
 }
 
 // --------------------------------------------------------------------------
-// build: initial star of every point from its candidate workset (at most
-// BUCKET_CAP + MIN_WORKSET points, so always the small class)
+// build: initial star of every point (list == null) or of the listed points
+// from its candidate workset (at most BUCKET_CAP + MIN_WORKSET points). A star
+// the small class cannot hold (a link of more than 64 points) is listed in
+// wlBig and built again in the large class.
 // --------------------------------------------------------------------------
 
-// 4 blocks per SM: shared memory (about 57 KB per block) allows no more, and
-// this register budget (128) costs only a few hundred bytes of spills.
-__global__ void __launch_bounds__(32 * WARPS_PER_BLOCK, 4) k_star_build(Dev D) {
+__device__ __forceinline__ void defer(int* list, int* counter, int s) {
+    const int q = atomicAdd(counter, 1);
+    list[q] = s;
+}
+
+template <class C, bool EXACT>
+__global__ void __launch_bounds__(32 * C::WARPS, EXACT ? C::MINB : C::MINB_FAST)
+    k_star_build(Dev D, const int* list, int count) {
     G4D_DYN_SMEM(smem_raw);
-    using C = SmallStar;
     const int lane = threadIdx.x & 31;
     WS<C>& S = reinterpret_cast<WS<C>*>(smem_raw)[threadIdx.x >> 5];
     const PredSink sink = sink_of(D);
     unsigned* err = sink.err;
     unsigned* exact = &D.ctr->exact;
-    const int warps = gridDim.x * WARPS_PER_BLOCK;
-    for (int s = blockIdx.x * WARPS_PER_BLOCK + (threadIdx.x >> 5); s < D.n; s += warps) {
+    const int warps = gridDim.x * C::WARPS;
+    for (int w = blockIdx.x * C::WARPS + (threadIdx.x >> 5); w < count; w += warps) {
+        const int s = list ? list[w] : w;
         __syncwarp();  // the previous star's shared-memory reads are done
         for (int k = lane; k < C::HS; k += 32) S.hh[k] = (int)HEMPTY;
         for (int k = lane; k < C::HS / 32; k += 32) { S.wasLink[k] = 0; S.insMask[k] = 0; }
@@ -700,14 +725,30 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK, 4) k_star_build(Dev D) {
         __syncwarp();
         const int gen = 1;
         int l4[4] = {S.order[0], S.order[1], S.order[2], S.order[3]};
-        warp_cone(S, lane, s, ps, l4, gen, sink, exact);
-        int failed = 0;
-        for (int i = 4; i < nins && !failed; ++i) {
-            const int r = warp_insert(S, lane, s, ps, S.order[i], gen, sink, exact);
-            if (r == -2 && lane == 0) atomicOr(err, ERR_CAPACITY);
-            failed = r < 0;
+        int r = warp_cone<C, EXACT>(S, lane, s, ps, l4, gen, sink, exact);
+        for (int i = 4; i < nins && r >= 0; ++i) r = warp_insert<C, EXACT>(S, lane, s, ps, S.order[i], gen, sink, exact);
+        if (r == -3 || r == -2) {
+            if (lane == 0) {
+                if (r == -3) defer(D.wlExact, &D.ctr->exact_next, s);
+                else if (!C::LARGE) defer(D.wlBig, &D.ctr->build_big, s);
+                else atomicOr(err, ERR_CAPACITY);
+            }
+            continue;
         }
-        if (failed) continue;
+        if (r < 0) continue;  // error flag raised
+        if (C::LARGE) {  // the star gets its large slot now
+            int li = 0;
+            if (lane == 0) {
+                li = atomicAdd(&D.ctr->large_next, 1);
+                if (li < D.largeCap) D.lidx[s] = li;
+            }
+            li = __shfl_sync(0xffffffffu, li, 0);
+            __syncwarp();
+            if (li >= D.largeCap) {
+                if (lane == 0) atomicOr(err, ERR_CAPACITY);
+                continue;
+            }
+        }
         warp_store(S, D, lane, s, gen, true);
         if (lane == 0) atomicAdd(&D.ctr->insertions, (unsigned long long)nins);
     }
@@ -718,8 +759,9 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK, 4) k_star_build(Dev D) {
 // its class keeps its inbox and joins the promotion list.
 // --------------------------------------------------------------------------
 
-template <class C>
-__global__ void __launch_bounds__(32 * C::WARPS, C::MINB) k_star_insert(Dev D, const int* list, int count) {
+template <class C, bool EXACT>
+__global__ void __launch_bounds__(32 * C::WARPS, EXACT ? C::MINB : C::MINB_FAST)
+    k_star_insert(Dev D, const int* list, int count) {
     G4D_DYN_SMEM(smem_raw);
     const int lane = threadIdx.x & 31;
     WS<C>& S = reinterpret_cast<WS<C>*>(smem_raw)[threadIdx.x >> 5];
@@ -752,18 +794,23 @@ __global__ void __launch_bounds__(32 * C::WARPS, C::MINB) k_star_insert(Dev D, c
         const int nins = S.nins;
         const int nhist0 = S.nhist;
         __syncwarp();  // all lanes read the counts before lane 0 updates them
-        bool outgrown = nhist0 + nins > C::HM;
+        bool outgrown = nhist0 + nins > C::HM, undecided = false;
         int any = 0, failed = 0;
         const int gen = (h.pass % 15) + 1;  // 1..15, differs from the stored pass
         if (!outgrown) {
             if (lane == 0) S.nhist = nhist0 + nins;
             __syncwarp();
             for (int i = 0; i < nins && !failed; ++i) {
-                const int r = warp_insert(S, lane, s, ps, S.order[i], gen, sink, exact);
+                const int r = warp_insert<C, EXACT>(S, lane, s, ps, S.order[i], gen, sink, exact);
                 outgrown = r == -2;
+                undecided = r == -3;
                 failed = r < 0;
                 any |= r > 0;
             }
+        }
+        if (undecided) {  // the exact kernel replays this star's round (inbox kept)
+            if (lane == 0) defer(D.wlExact, &D.ctr->exact_next, s);
+            continue;
         }
         if (outgrown) {
             if (lane == 0) {
@@ -1270,26 +1317,32 @@ static int star_blocks(int items, int warps_per_block = WARPS_PER_BLOCK, int per
     return b < 1 ? 1 : b;
 }
 
-void launch_star_build(const Launch& L, const Dev& D) {
-    const size_t sm = sizeof(WS<SmallStar>) * WARPS_PER_BLOCK;
-    cudaFuncSetAttribute(k_star_build, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_star_build<<<star_blocks(D.n), 32 * WARPS_PER_BLOCK, sm, L.stream>>>(D);
+template <class C, bool EXACT, class K>
+static void launch_star(const Launch& L, K kernel, const Dev& D, const int* list, int count) {
+    const size_t sm = sizeof(WS<C>) * C::WARPS;
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    const int per_sm = C::LARGE ? 1 : 8;
+    kernel<<<star_blocks(count, C::WARPS, per_sm), 32 * C::WARPS, sm, L.stream>>>(D, list, count);
     ++*L.launches;
 }
 
-void launch_star_insert(const Launch& L, const Dev& D, int count) {
-    const size_t sm = sizeof(WS<SmallStar>) * SmallStar::WARPS;
-    cudaFuncSetAttribute(k_star_insert<SmallStar>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_star_insert<SmallStar><<<star_blocks(count), 32 * SmallStar::WARPS, sm, L.stream>>>(D, D.wlIns, count);
-    ++*L.launches;
+void launch_star_build(const Launch& L, const Dev& D, const int* list, int count, bool exact) {
+    const int c = list ? count : D.n;
+    if (exact) launch_star<SmallStar, true>(L, k_star_build<SmallStar, true>, D, list, c);
+    else launch_star<SmallStar, false>(L, k_star_build<SmallStar, false>, D, list, c);
+}
+
+void launch_star_build_large(const Launch& L, const Dev& D, const int* list, int count) {
+    launch_star<LargeStar, true>(L, k_star_build<LargeStar, true>, D, list, count);
+}
+
+void launch_star_insert(const Launch& L, const Dev& D, const int* list, int count, bool exact) {
+    if (exact) launch_star<SmallStar, true>(L, k_star_insert<SmallStar, true>, D, list, count);
+    else launch_star<SmallStar, false>(L, k_star_insert<SmallStar, false>, D, list, count);
 }
 
 void launch_star_insert_large(const Launch& L, const Dev& D, const int* list, int count) {
-    const size_t sm = sizeof(WS<LargeStar>) * LargeStar::WARPS;
-    cudaFuncSetAttribute(k_star_insert<LargeStar>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_star_insert<LargeStar><<<star_blocks(count, LargeStar::WARPS, 1), 32 * LargeStar::WARPS, sm, L.stream>>>(
-        D, list, count);
-    ++*L.launches;
+    launch_star<LargeStar, true>(L, k_star_insert<LargeStar, true>, D, list, count);
 }
 
 void launch_promote(const Launch& L, const Dev& D, int count) {
