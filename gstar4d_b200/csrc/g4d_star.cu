@@ -25,6 +25,9 @@
 namespace g4d {
 
 constexpr int WARPS_PER_BLOCK = 4;
+#ifndef FAST_BLOCKS
+#define FAST_BLOCKS 8  // blocks per SM of the filter-only star kernels
+#endif
 
 // ---------------------------------------------------------------------------
 // storage classes
@@ -32,10 +35,11 @@ constexpr int WARPS_PER_BLOCK = 4;
 
 struct SmallStar {
     static constexpr int LOG2_HS = 8, HS = HSLOTS, HM = HMAX, TM = TMAX, TS = TSTRIDE;
-    // blocks per SM: 6 filter-only (about 80 registers), 4 with the exact path
-    static constexpr int WARPS = WARPS_PER_BLOCK, MINB = 4, MINB_FAST = 6;
+    // blocks per SM: FAST_BLOCKS filter-only (64 registers at 8), 4 with the exact path
+    static constexpr int WARPS = WARPS_PER_BLOCK, MINB = 4, MINB_FAST = FAST_BLOCKS;
     static constexpr bool LARGE = false;
     using Idx = uint8_t;   // triangle index and coordinate-cache index
+    using Slot = uint8_t;  // history slot
     using Rec = uint32_t;  // hole boundary edge: u | w<<9 | o<<18 | oj<<26
     using Tri = uint2;     // packing in g4d_internal.cuh
     __device__ static Rec rec(int u, int w, int o, int oj) {
@@ -65,6 +69,7 @@ struct LargeStar {
     static constexpr int WARPS = 1, MINB = 1, MINB_FAST = 1;  // about 141 KB of shared memory per warp
     static constexpr bool LARGE = true;
     using Idx = uint16_t;
+    using Slot = uint16_t;
     using Rec = unsigned long long;  // u | w<<12 | o<<24 | oj<<35
     using Tri = uint4;
     __device__ static Rec rec(int u, int w, int o, int oj) {
@@ -103,7 +108,7 @@ struct WS {
     int hh[C::HS];                 // history hash: point id | link bit, HEMPTY when free
     Idx cix[C::HS];                // slot -> index into the coordinate cache
     double cx[C::HM + 1], cy[C::HM + 1], cz[C::HM + 1];
-    uint16_t tv[3][C::TS];         // triangle vertices (history slots)
+    typename C::Slot tv[3][C::TS];  // triangle vertices (history slots)
     Idx to[3][C::TS];              // neighbour across the edge opposite each vertex
     uint8_t tj[3][C::TS];          // position of the shared edge inside that neighbour
     uint8_t tf[C::TS];             // bit 7 alive, bits 0..3 creation pass
@@ -114,7 +119,7 @@ struct WS {
     };
     Idx blist[C::TS];              // beneath triangles in index order / compaction map
     Idx fstack[C::TS];             // free triangle slots
-    uint16_t order[C::HM + 1];     // insertion order (slots)
+    typename C::Slot order[C::HM + 1];  // insertion order (slots)
     uint32_t bmask[C::TS / 32];
     uint32_t wasLink[C::HS / 32], insMask[C::HS / 32];
     int nedge, nfree, ntri, nins, nhist, ncoord;
@@ -431,9 +436,9 @@ __device__ int warp_insert(WS<C>& S, int lane, int s, double3 ps, int sp, int ge
         const typename C::Rec e = S.erec[r];
         const int u = C::rec_u(e), w = C::rec_w(e), o = C::rec_o(e), oj = C::rec_oj(e);
         const int slot = S.efrom[S.cix[u]];
-        S.tv[0][slot] = (uint16_t)u;
-        S.tv[1][slot] = (uint16_t)w;
-        S.tv[2][slot] = (uint16_t)sp;
+        S.tv[0][slot] = (typename C::Slot)u;
+        S.tv[1][slot] = (typename C::Slot)w;
+        S.tv[2][slot] = (typename C::Slot)sp;
         S.to[0][slot] = S.efrom[S.cix[w]];  // edge (w, p): the next boundary edge's triangle
         S.tj[0][slot] = 1;
         S.to[1][slot] = S.eto[S.cix[u]];    // edge (p, u): the previous boundary edge's triangle
@@ -482,7 +487,7 @@ __device__ int warp_cone(WS<C>& S, int lane, int s, double3 ps, const int* l4, i
         const int F[4][3] = {{1, 2, 3}, {0, 3, 2}, {0, 1, 3}, {0, 2, 1}};
         const int f = lane;
         for (int i = 0; i < 3; ++i) {
-            S.tv[i][f] = (uint16_t)l[F[f][i]];
+            S.tv[i][f] = (typename C::Slot)l[F[f][i]];
             const int b = F[f][i];  // the face omitting vertex F[f][i] shares this edge
             S.to[i][f] = (typename C::Idx)b;
             int j = 0;
@@ -516,7 +521,7 @@ __device__ void warp_sort_order(WS<C>& S, int lane, int n) {
                     const float a = S.okey[i], b = S.okey[p];
                     if ((a > b) == up) {
                         S.okey[i] = b; S.okey[p] = a;
-                        const uint16_t t = S.order[i]; S.order[i] = S.order[p]; S.order[p] = t;
+                        const auto t = S.order[i]; S.order[i] = S.order[p]; S.order[p] = t;
                     }
                 }
             }
@@ -547,7 +552,7 @@ __device__ void warp_load(WS<C>& S, const Dev& D, int lane, int s, StarHdr h) {
         const typename C::Tri T = gt[t];
 #pragma unroll
         for (int i = 0; i < 3; ++i) {
-            S.tv[i][t] = (uint16_t)C::tv(T, i);
+            S.tv[i][t] = (typename C::Slot)C::tv(T, i);
             S.to[i][t] = (Idx)C::to(T, i);
             S.tj[i][t] = (uint8_t)C::tj(T, i);
         }
@@ -663,7 +668,7 @@ __global__ void __launch_bounds__(32 * C::WARPS, EXACT ? C::MINB : C::MINB_FAST)
             const int slot = ws_hash_insert(S, v, &fresh);
             if (fresh) {
                 const int pos = atomicAdd(&S.nins, 1);
-                S.order[pos] = (uint16_t)slot;
+                S.order[pos] = (typename C::Slot)slot;
             }
         }
         __syncwarp();
@@ -682,7 +687,7 @@ __global__ void __launch_bounds__(32 * C::WARPS, EXACT ? C::MINB : C::MINB_FAST)
                         if (v == s || !valid_id(D, v)) continue;
                         bool fresh;
                         const int slot = ws_hash_insert(S, v, &fresh);
-                        if (fresh) S.order[have++] = (uint16_t)slot;
+                        if (fresh) S.order[have++] = (typename C::Slot)slot;
                     }
                 }
                 int lo, hi;
@@ -691,7 +696,7 @@ __global__ void __launch_bounds__(32 * C::WARPS, EXACT ? C::MINB : C::MINB_FAST)
                     if (v == s) continue;
                     bool fresh;
                     const int slot = ws_hash_insert(S, v, &fresh);
-                    if (fresh) S.order[have++] = (uint16_t)slot;
+                    if (fresh) S.order[have++] = (typename C::Slot)slot;
                 }
                 // reciprocal requests for the pumped points
                 bool ovf = false;
@@ -785,7 +790,7 @@ __global__ void __launch_bounds__(32 * C::WARPS, EXACT ? C::MINB : C::MINB_FAST)
             if (slot < 0) { atomicOr(err, ERR_CAPACITY); continue; }
             if (fresh) {
                 const int pos = atomicAdd(&S.nins, 1);
-                S.order[pos < C::HM ? pos : C::HM] = (uint16_t)slot;
+                S.order[pos < C::HM ? pos : C::HM] = (typename C::Slot)slot;
                 ws_cache_coords(S, D, slot, v);
                 atomicOr(&S.insMask[slot >> 5], 1u << (slot & 31));
             }
