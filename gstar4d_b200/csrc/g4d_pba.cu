@@ -152,14 +152,24 @@ __global__ void __launch_bounds__(256) k_pba_x(int G, const uint32_t* __restrict
 }
 
 
-constexpr int PAIR_HASH = 4096;
+#ifndef PAIR_HASH_LOG2
+#define PAIR_HASH_LOG2 11
+#endif
+#ifndef PAIR_ZC_DEF
+#define PAIR_ZC_DEF 16
+#endif
+#ifndef PAIR_WARPS_DEF
+#define PAIR_WARPS_DEF 4
+#endif
+constexpr int PAIR_HASH = 1 << PAIR_HASH_LOG2;  // block hash entries (8 bytes each)
 constexpr int PAIR_PROBES = 32;
-constexpr int PAIR_ZC = 16;
+constexpr int PAIR_ZC = PAIR_ZC_DEF;            // cube planes per block
+constexpr int PAIR_WARPS = PAIR_WARPS_DEF;      // warps per block, one row of x each
 
 template <class KeyT>
 __device__ __forceinline__ void pair_hash_insert(unsigned long long* hs, unsigned long long key, const Dev& D,
                                                  const Cols<KeyT>& C) {
-    unsigned h = (unsigned)((key * 0x9E3779B97F4A7C15ull) >> 52) & (PAIR_HASH - 1);
+    unsigned h = (unsigned)((key * 0x9E3779B97F4A7C15ull) >> (64 - PAIR_HASH_LOG2));
     for (int probe = 0; probe < PAIR_PROBES; ++probe) {
         const unsigned long long old = atomicCAS(&hs[h], ~0ull, key);
         if (old == ~0ull || old == key) return;
@@ -175,12 +185,15 @@ __device__ __forceinline__ void pair_hash_insert(unsigned long long* hs, unsigne
 // which at least four sites meet (a digital Voronoi vertex: its sites are
 // pairwise Voronoi neighbours; the reference reads the same cubes and emits
 // around digital Voronoi vertices, GDelKernels.cu:137-299). One thread sweeps a
-// column of cubes along z, keeping the previous voxel plane in registers (4 new
-// loads per cube, coalesced over x). Vertex cubes are rare: a lane queues the
-// site set of each one (skipping a repeat of its previous set) in a per-warp
-// queue, and every 32 queued cubes the warp emits their pairs, one cube per
-// lane, into a block-local hash that removes duplicates before the per-star
-// scatter.
+// column of cubes along z, keeping the previous voxel plane in registers and
+// loading the plane after the next one ahead of use (4 loads per cube,
+// coalesced over x). The distinct sites of a cube are a bit mask computed
+// without branches (bit i: voxel i differs from voxels 0..i-1), so every lane
+// does the same few dozen instructions per cube. Vertex cubes are rare (about
+// 5% of the cubes): a lane queues the site set of each one (skipping a repeat
+// of its previous set) in a per-warp queue, and every 32 queued cubes the warp
+// emits their pairs, one cube per lane, into a block-local hash that removes
+// duplicates before the per-star scatter.
 // all pairs of one queued vertex cube into the block hash
 template <class KeyT>
 __device__ __forceinline__ void emit_cube(unsigned long long* hs, const uint32_t* q, int ns, const Dev& D,
@@ -194,17 +207,30 @@ __device__ __forceinline__ void emit_cube(unsigned long long* hs, const uint32_t
 
 constexpr int PAIR_QUEUE = 64;  // queued vertex cubes per warp
 
+// bit i set when v[i] differs from v[0..i-1]; v[0..3] is the lower plane
+__device__ __forceinline__ uint32_t distinct_mask(const uint32_t (&v)[8]) {
+    uint32_t m = 1u;
+#pragma unroll
+    for (int i = 1; i < 8; ++i) {
+        bool fresh = true;
+#pragma unroll
+        for (int j = 0; j < i; ++j) fresh = fresh && (v[i] != v[j]);
+        m |= (uint32_t)fresh << i;
+    }
+    return m;
+}
+
 template <class KeyT>
-__global__ void __launch_bounds__(128) k_pairs(Dev D, const uint32_t* __restrict__ stack, Cols<KeyT> C, int nzc) {
+__global__ void __launch_bounds__(32 * PAIR_WARPS) k_pairs(Dev D, const uint32_t* __restrict__ stack, Cols<KeyT> C, int nzc) {
     __shared__ unsigned long long hs[PAIR_HASH];
-    __shared__ uint32_t qs[4][PAIR_QUEUE][8];  // site sets of vertex cubes
-    __shared__ uint8_t qn[4][PAIR_QUEUE];
+    __shared__ uint32_t qs[PAIR_WARPS][PAIR_QUEUE][8];  // site sets of vertex cubes
+    __shared__ uint8_t qn[PAIR_WARPS][PAIR_QUEUE];
     const int G = C.G;
     const int tid = threadIdx.y * 32 + threadIdx.x;
-    for (int k = tid; k < PAIR_HASH; k += 128) hs[k] = ~0ull;
+    for (int k = tid; k < PAIR_HASH; k += 32 * PAIR_WARPS) hs[k] = ~0ull;
     __syncthreads();
     const int x = blockIdx.x * 32 + threadIdx.x;
-    const int y = blockIdx.y * 4 + threadIdx.y;
+    const int y = blockIdx.y * PAIR_WARPS + threadIdx.y;
     const int kk = blockIdx.z / nzc;  // grid of the stack
     const int z0 = (blockIdx.z - kk * nzc) * PAIR_ZC;
     const size_t plane = (size_t)G * G;
@@ -213,48 +239,59 @@ __global__ void __launch_bounds__(128) k_pairs(Dev D, const uint32_t* __restrict
     C.end += (size_t)kk * plane;
     const int lane = threadIdx.x, w = threadIdx.y;
     // every lane of the warp walks the same z range so the warp collectives
-    // below stay converged; lanes past the grid edge carry no pairs
+    // below stay converged; lanes past the grid edge carry no pairs (they read
+    // column 0, which is in bounds)
     const bool active = x < G - 1 && y < G - 1;
     const int zend = min(z0 + PAIR_ZC, G - 1);
     if (y < G - 1 && z0 < G - 1) {
         const uint32_t* g = grid + (size_t)y * G + (active ? x : 0);
-        uint32_t a0 = g[(size_t)z0 * plane], a1 = g[(size_t)z0 * plane + 1];
-        uint32_t a2 = g[(size_t)z0 * plane + G], a3 = g[(size_t)z0 * plane + G + 1];
+        uint32_t v[8];
+        {
+            const size_t o = (size_t)z0 * plane;
+            v[0] = g[o]; v[1] = g[o + 1]; v[2] = g[o + G]; v[3] = g[o + G + 1];
+        }
+        // plane z0+1 exists: z0 < G-1
+        uint32_t n0, n1, n2, n3;
+        {
+            const size_t o = (size_t)(z0 + 1) * plane;
+            n0 = g[o]; n1 = g[o + 1]; n2 = g[o + G]; n3 = g[o + G + 1];
+        }
         unsigned long long last = 0;  // signature of the set this lane queued last
         int qc = 0;                   // queued cubes of this warp (same in every lane)
         for (int z = z0; z < zend; ++z) {
-            const size_t o = (size_t)(z + 1) * plane;
-            const uint32_t b0 = g[o], b1 = g[o + 1], b2 = g[o + G], b3 = g[o + G + 1];
+            v[4] = n0; v[5] = n1; v[6] = n2; v[7] = n3;
+            if (z + 1 < zend) {  // the plane after the next one, loaded ahead of use
+                const size_t o = (size_t)(z + 2) * plane;
+                n0 = g[o]; n1 = g[o + 1]; n2 = g[o + G]; n3 = g[o + G + 1];
+            }
             bool cand = false;
-            uint32_t sset[8];
-            int ns = 0;
-            // most cubes lie inside one Voronoi cell: four sites need at least
-            // three voxels that differ from a0
-            const int diff = (a1 != a0) + (a2 != a0) + (a3 != a0) + (b0 != a0) + (b1 != a0) + (b2 != a0) + (b3 != a0);
-            if (active && diff >= 3) {
-                const uint32_t v[8] = {a0, a1, a2, a3, b0, b1, b2, b3};
-#pragma unroll
-                for (int i = 0; i < 8; ++i) {
-                    bool dup = false;
-                    for (int k = 0; k < ns; ++k) dup |= (sset[k] == v[i]);
-                    if (!dup) sset[ns++] = v[i];
-                }
-                if (ns >= 4) {
+            uint32_t m = 0;
+            // a warp whose cubes all lie inside one Voronoi cell each skips the mask
+            const bool mixed = (v[1] != v[0]) | (v[2] != v[0]) | (v[3] != v[0]) | (v[4] != v[0]) |
+                               (v[5] != v[0]) | (v[6] != v[0]) | (v[7] != v[0]);
+            if (__any_sync(0xffffffffu, active && mixed)) {
+                m = distinct_mask(v);
+                if (active && __popc(m) >= 4) {
                     // consecutive cubes around one Voronoi vertex repeat its set
                     unsigned long long sum = 0, xr = 0;
-                    for (int k = 0; k < ns; ++k) { sum += sset[k]; xr ^= (unsigned long long)sset[k] * 0x9E3779B97F4A7C15ull; }
-                    const unsigned long long sig = (sum << 32) ^ xr ^ (unsigned long long)ns;
+#pragma unroll
+                    for (int k = 0; k < 8; ++k)
+                        if (m >> k & 1u) { sum += v[k]; xr ^= (unsigned long long)v[k] * 0x9E3779B97F4A7C15ull; }
+                    const unsigned long long sig = (sum << 32) ^ xr ^ (unsigned long long)__popc(m);
                     cand = sig != last;
                     last = sig;
                 }
             }
-            const unsigned m = __ballot_sync(0xffffffffu, cand);
+            const unsigned bal = __ballot_sync(0xffffffffu, cand);
             if (cand) {
-                const int pos = qc + __popc(m & ((1u << lane) - 1u));
-                for (int k = 0; k < ns; ++k) qs[w][pos][k] = sset[k];
+                const int pos = qc + __popc(bal & ((1u << lane) - 1u));
+                int ns = 0;
+#pragma unroll
+                for (int k = 0; k < 8; ++k)
+                    if (m >> k & 1u) qs[w][pos][ns++] = v[k];
                 qn[w][pos] = (uint8_t)ns;
             }
-            qc += __popc(m);
+            qc += __popc(bal);
             if (qc >= 32) {  // one queued cube per lane
                 __syncwarp();
                 emit_cube(hs, qs[w][lane], qn[w][lane], D, C);
@@ -266,13 +303,13 @@ __global__ void __launch_bounds__(128) k_pairs(Dev D, const uint32_t* __restrict
                 qc -= 32;
                 __syncwarp();
             }
-            a0 = b0; a1 = b1; a2 = b2; a3 = b3;
+            v[0] = v[4]; v[1] = v[5]; v[2] = v[6]; v[3] = v[7];
         }
         __syncwarp();
         if (lane < qc) emit_cube(hs, qs[w][lane], qn[w][lane], D, C);
     }
     __syncthreads();
-    for (int k = tid; k < PAIR_HASH; k += 128) {
+    for (int k = tid; k < PAIR_HASH; k += 32 * PAIR_WARPS) {
         const unsigned long long key = hs[k];
         if (key == ~0ull) continue;
         const int ia = site_to_id(C, (uint32_t)(key >> 32)), ib = site_to_id(C, (uint32_t)key);
@@ -351,7 +388,7 @@ void launch_pba_x_stack(const Launch& L, int G, int K, const uint32_t* in, uint3
 void launch_pairs(const Launch& L, const Dev& D, const uint32_t* grid) {
     const int G = D.G;
     const int nzc = (G - 1 + PAIR_ZC - 1) / PAIR_ZC;
-    dim3 b(32, 4), g((G - 1 + 31) / 32, (G - 1 + 3) / 4, nzc);
+    dim3 b(32, PAIR_WARPS), g((G - 1 + 31) / 32, (G - 1 + PAIR_WARPS - 1) / PAIR_WARPS, nzc);
     k_pairs<<<g, b, 0, L.stream>>>(D, grid, Cols<uint32_t>{D.ckey, D.cid, D.colStart, D.colEnd, G}, nzc);
     ++*L.launches;
 }
@@ -359,7 +396,7 @@ void launch_pairs(const Launch& L, const Dev& D, const uint32_t* grid) {
 void launch_pairs_stack(const Launch& L, const Dev& D, const uint32_t* stack, int G, int K,
                         const unsigned long long* ckey, const int* cid, const int* cs, const int* ce) {
     const int nzc = (G - 1 + PAIR_ZC - 1) / PAIR_ZC;
-    dim3 b(32, 4), g((G - 1 + 31) / 32, (G - 1 + 3) / 4, nzc * K);
+    dim3 b(32, PAIR_WARPS), g((G - 1 + 31) / 32, (G - 1 + PAIR_WARPS - 1) / PAIR_WARPS, nzc * K);
     k_pairs<<<g, b, 0, L.stream>>>(D, stack, Cols<unsigned long long>{ckey, cid, cs, ce, G}, nzc);
     ++*L.launches;
 }
