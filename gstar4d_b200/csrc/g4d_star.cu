@@ -1041,16 +1041,23 @@ __device__ __forceinline__ int find_tri_t(const int* h, const typename C::Tri* g
                                           bool cyclic) {
     const int sx = hash_slot<C>(h, x), sy = hash_slot<C>(h, y), sz = hash_slot<C>(h, z);
     if (sx < 0 || sy < 0 || sz < 0) return -1;
-    for (int t = 0; t < ntri; ++t) {
-        const typename C::Tri T = gt[t];
-        const int a = C::tv(T, 0), b = C::tv(T, 1), c = C::tv(T, 2);
-        if (cyclic) {
-            if ((a == sx && b == sy && c == sz) || (b == sx && c == sy && a == sz) || (c == sx && a == sy && b == sz))
-                return t;
-        } else {
-            const bool hx = a == sx || b == sx || c == sx, hy = a == sy || b == sy || c == sy,
-                       hz = a == sz || b == sz || c == sz;
-            if (hx && hy && hz) return t;
+    // four triangles per step, loaded together (clamped to the last one)
+    for (int t0 = 0; t0 < ntri; t0 += 4) {
+        typename C::Tri T[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) T[u] = gt[min(t0 + u, ntri - 1)];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int a = C::tv(T[u], 0), b = C::tv(T[u], 1), c = C::tv(T[u], 2);
+            bool hit;
+            if (cyclic) {
+                hit = (a == sx && b == sy && c == sz) || (b == sx && c == sy && a == sz) ||
+                      (c == sx && a == sy && b == sz);
+            } else {
+                hit = (a == sx || b == sx || c == sx) && (a == sy || b == sy || c == sy) &&
+                      (a == sz || b == sz || c == sz);
+            }
+            if (hit && t0 + u < ntri) return t0 + u;
         }
     }
     return -1;
@@ -1120,27 +1127,35 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_tet_count(Dev D, int* 
     }
 }
 
+// tet id of triangle ti of `star` when it is kept (a tetrahedron owned by the
+// star), else -1
+__device__ __forceinline__ int kept_tet_id(const Dev& D, const int* base, int star, const StarView& V, int ti) {
+    if (!V.large) {
+        const uint32_t* m = D.keptMask + (size_t)star * (TSTRIDE / 32);
+        const uint4 mw = *reinterpret_cast<const uint4*>(m);  // TSTRIDE / 32 == 4 words
+        const uint32_t w[4] = {mw.x, mw.y, mw.z, mw.w};
+        const int q = ti >> 5;
+        const uint32_t cur = q == 0 ? w[0] : (q == 1 ? w[1] : (q == 2 ? w[2] : w[3]));
+        if (!((cur >> (ti & 31)) & 1u)) return -1;
+        int r = __popc(cur & ((1u << (ti & 31)) - 1u));
+        r += (q > 0 ? __popc(w[0]) : 0) + (q > 1 ? __popc(w[1]) : 0) + (q > 2 ? __popc(w[2]) : 0);
+        return base[star] + r;
+    }
+    if (!tri_kept(V, ti)) return -1;
+    int r = 0;
+    for (int t = 0; t < ti; ++t) r += tri_kept(V, t);
+    return base[star] + r;
+}
+
 // tet id of the kept tetrahedron owned by `star` (its smallest vertex) whose
 // other vertices are {x,y,z}, or -1
 __device__ int owned_tet_id(const Dev& D, const int* base, int star, int x, int y, int z) {
     if (!valid_id(D, star)) return -1;
     const StarView V = star_view(D, star);
     const int ntri = D.hdr[star].ntri;
-    if (!V.large) {
-        const int ti = find_tri_t<SmallStar>(V.hh, static_cast<const uint2*>(V.tri), ntri, x, y, z, false);
-        if (ti < 0) return -1;
-        const uint32_t* m = D.keptMask + (size_t)star * (TSTRIDE / 32);
-        const uint32_t mw = m[ti >> 5];
-        if (!((mw >> (ti & 31)) & 1u)) return -1;
-        int r = __popc(mw & ((1u << (ti & 31)) - 1u));
-        for (int w = 0; w < (ti >> 5); ++w) r += __popc(m[w]);
-        return base[star] + r;
-    }
-    const int ti = find_tri_t<LargeStar>(V.hh, static_cast<const uint4*>(V.tri), ntri, x, y, z, false);
-    if (ti < 0 || !tri_kept(V, ti)) return -1;
-    int r = 0;
-    for (int t = 0; t < ti; ++t) r += tri_kept(V, t);
-    return base[star] + r;
+    const int ti = V.large ? find_tri_t<LargeStar>(V.hh, static_cast<const uint4*>(V.tri), ntri, x, y, z, false)
+                           : find_tri_t<SmallStar>(V.hh, static_cast<const uint2*>(V.tri), ntri, x, y, z, false);
+    return ti < 0 ? -1 : kept_tet_id(D, base, star, V, ti);
 }
 
 // the vertex y beyond edge (b,c) from s in star a: the triangle (b, s, c) of
@@ -1162,21 +1177,41 @@ __device__ __forceinline__ int across_t(const int* h, const typename C::Tri* gt,
     return y;
 }
 
-// neighbour of tetrahedron (a, b, c, s) across the face (a, b, c), or -1
-__device__ int face_neighbor(const Dev& D, const int* base, int s, int a, int b, int c) {
-    if (!valid_id(D, a)) return -1;
-    const StarView Va = star_view(D, a);
-    const int ntri = D.hdr[a].ntri;
-    const int y = Va.large ? across_t<LargeStar>(Va.hh, static_cast<const uint4*>(Va.tri), ntri, s, b, c)
-                           : across_t<SmallStar>(Va.hh, static_cast<const uint2*>(Va.tri), ntri, s, b, c);
-    if (y < 0) return -1;
-    const int all4[4] = {a, b, c, y};
-    int m = a;
-    for (int k = 1; k < 4; ++k) m = all4[k] < m ? all4[k] : m;
-    int q[3], nq = 0;
-    for (int k = 0; k < 4; ++k)
-        if (all4[k] != m && nq < 3) q[nq++] = all4[k];
-    return nq == 3 ? owned_tet_id(D, base, m, q[0], q[1], q[2]) : -1;
+// star m's triangle {a, s, b} and the triangle beyond its edge (a, b): returns
+// the index of that neighbour triangle and sets *y to its third vertex; -1 if
+// absent
+template <class C>
+__device__ __forceinline__ int across_t(const int* h, const typename C::Tri* gt, int ntri, int s, int a, int b,
+                                        int* y) {
+    const int ta = find_tri_t<C>(h, gt, ntri, a, s, b, false);
+    if (ta < 0) return -1;
+    const typename C::Tri A = gt[ta];
+    const int i0 = h[C::tv(A, 0)] & (int)HID, i1 = h[C::tv(A, 1)] & (int)HID;
+    const int pos = i0 == s ? 0 : (i1 == s ? 1 : 2);
+    const int ni = C::to(A, pos);
+    const typename C::Tri N = gt[ni];
+    const int n0 = h[C::tv(N, 0)] & (int)HID, n1 = h[C::tv(N, 1)] & (int)HID, n2 = h[C::tv(N, 2)] & (int)HID;
+    *y = (n2 != a && n2 != b) ? n2 : ((n1 != a && n1 != b) ? n1 : n0);
+    return ni;
+}
+
+// neighbour of tetrahedron (v0, v1, v2, s), s its smallest vertex, across the
+// face (v0, v1, v2), or -1. It is found through m, the smallest of v0, v1, v2:
+// the link triangle {a, s, b} of star m and the link triangle beyond its edge
+// (a, b), {a, b, y}, which is the neighbour itself (owned by m) when y > m;
+// otherwise the neighbour is owned by y.
+__device__ int face_neighbor(const Dev& D, const int* base, int s, int v0, int v1, int v2) {
+    const int m = min(v0, min(v1, v2));
+    const int a = m == v0 ? v1 : v0, b = m == v2 ? v1 : v2;
+    if (!valid_id(D, m)) return -1;
+    const StarView V = star_view(D, m);
+    const int ntri = D.hdr[m].ntri;
+    int y = -1;
+    const int ni = V.large ? across_t<LargeStar>(V.hh, static_cast<const uint4*>(V.tri), ntri, s, a, b, &y)
+                           : across_t<SmallStar>(V.hh, static_cast<const uint2*>(V.tri), ntri, s, a, b, &y);
+    if (ni < 0) return -1;
+    if (y > m) return kept_tet_id(D, base, m, V, ni);
+    return owned_tet_id(D, base, y, m, a, b);
 }
 
 // tetrahedra owned by star s (a warp)
@@ -1227,10 +1262,80 @@ __device__ __forceinline__ void write_star(const Dev& D, const int* base, g4d_te
     }
 }
 
+// tetrahedra owned by small star s (a warp), one neighbour per lane: the kept
+// triangles are listed by rank, then lane k finds neighbour k&3 of tetrahedron
+// k>>2 (about 27 lookups per star, so most lanes work at once and a star costs
+// about one remote lookup of latency instead of four), then each lane writes
+// whole tetrahedra. buf: 128 B ranks, 128 B kept list, 4 ints per kept triangle.
+__device__ __forceinline__ void write_star_small(const Dev& D, const int* base, g4d_tet* tets,
+                                                 const int* sorted_to_input, int s, int ntri, const int* ids,
+                                                 const uint2* gt, uint8_t* buf, int lane) {
+    uint8_t* rank = buf;
+    uint8_t* kt = buf + 128;
+    int* opp = reinterpret_cast<int*>(buf + 256);
+    int nk = 0;
+    for (int b0 = 0; b0 < ntri; b0 += 32) {
+        const int t = b0 + lane;
+        const bool kept = t < ntri && SmallStar::kept(gt[t]);
+        const unsigned m = __ballot_sync(0xffffffffu, kept);
+        const int r = nk + __popc(m & ((1u << lane) - 1u));
+        if (t < ntri) rank[t] = (uint8_t)r;
+        if (kept) kt[r] = (uint8_t)t;
+        nk += __popc(m);
+    }
+    __syncwarp();
+    const int bs = base[s];
+    for (int k = lane; k < 4 * nk; k += 32) {
+        const int f = k & 3;
+        const uint2 T = gt[kt[k >> 2]];
+        const int s0 = SmallStar::tv(T, 0), s1 = SmallStar::tv(T, 1), s2 = SmallStar::tv(T, 2);
+        const int v0 = ids[s0] & (int)HID, v1 = ids[s1] & (int)HID, v2 = ids[s2] & (int)HID;
+        int o;
+        if (f < 3) {
+            // across the face (s, v[f+1], v[f+2]): the adjacent link triangle
+            const int oi = SmallStar::to(T, f);
+            const uint2 N = gt[oi];
+            const int e1 = f == 0 ? s1 : (f == 1 ? s2 : s0), e2 = f == 0 ? s2 : (f == 1 ? s0 : s1);
+            const int n0 = SmallStar::tv(N, 0), n1 = SmallStar::tv(N, 1), n2 = SmallStar::tv(N, 2);
+            const int xs = (n2 != e1 && n2 != e2) ? n2 : ((n1 != e1 && n1 != e2) ? n1 : n0);
+            const int x = ids[xs] & (int)HID;
+            if (x > s)
+                o = SmallStar::kept(N) ? bs + rank[oi] : -1;
+            else
+                o = owned_tet_id(D, base, x, s, f == 0 ? v1 : (f == 1 ? v2 : v0), f == 0 ? v2 : (f == 1 ? v0 : v1));
+        } else {
+            o = face_neighbor(D, base, s, v0, v1, v2);
+        }
+        opp[k] = o;
+    }
+    __syncwarp();
+    for (int r = lane; r < nk; r += 32) {
+        const uint2 T = gt[kt[r]];
+        const int v0 = ids[SmallStar::tv(T, 0)] & (int)HID, v1 = ids[SmallStar::tv(T, 1)] & (int)HID,
+                  v2 = ids[SmallStar::tv(T, 2)] & (int)HID;
+        g4d_tet out;
+        if (sorted_to_input) {
+            out.v[0] = sorted_to_input[v0];
+            out.v[1] = sorted_to_input[v1];
+            out.v[2] = sorted_to_input[v2];
+            out.v[3] = sorted_to_input[s];
+        } else {
+            out.v[0] = v0; out.v[1] = v1; out.v[2] = v2; out.v[3] = s;
+        }
+        out.opp[0] = opp[4 * r];
+        out.opp[1] = opp[4 * r + 1];
+        out.opp[2] = opp[4 * r + 2];
+        out.opp[3] = opp[4 * r + 3];
+        tets[bs + r] = out;
+    }
+}
+
 __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_tet_write(Dev D, const int* base, g4d_tet* tets,
                                                                     const int* sorted_to_input) {
     __shared__ int shh[WARPS_PER_BLOCK][HSLOTS];
-    __shared__ uint16_t srank[WARPS_PER_BLOCK][LTSTRIDE];
+    // large stars: triangle ranks; small stars: write_star_small's buffer
+    __shared__ __align__(16) uint16_t srank[WARPS_PER_BLOCK][LTSTRIDE];
+    static_assert(256 + 4 * TMAX * sizeof(int) <= LTSTRIDE * sizeof(uint16_t), "small-star output buffer");
     const int lane = threadIdx.x & 31;
     uint16_t* rank = srank[threadIdx.x >> 5];
     const int warps = gridDim.x * WARPS_PER_BLOCK;
@@ -1240,8 +1345,8 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_tet_write(Dev D, const
         const StarView V = star_view(D, s);
         const int* ids = stage_ids(V, shh[threadIdx.x >> 5], lane);
         if (!V.large)
-            write_star<SmallStar>(D, base, tets, sorted_to_input, s, h.ntri, ids, static_cast<const uint2*>(V.tri),
-                                  rank, lane);
+            write_star_small(D, base, tets, sorted_to_input, s, h.ntri, ids, static_cast<const uint2*>(V.tri),
+                             reinterpret_cast<uint8_t*>(rank), lane);
         else
             write_star<LargeStar>(D, base, tets, sorted_to_input, s, h.ntri, ids, static_cast<const uint4*>(V.tri),
                                   rank, lane);
