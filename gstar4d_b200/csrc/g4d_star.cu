@@ -28,6 +28,9 @@ constexpr int WARPS_PER_BLOCK = 4;
 #ifndef FAST_BLOCKS
 #define FAST_BLOCKS 8  // blocks per SM of the filter-only star kernels
 #endif
+#ifndef PROOF_BLOCKS
+#define PROOF_BLOCKS 8  // blocks per SM of the filter-only proof kernel
+#endif
 
 // ---------------------------------------------------------------------------
 // storage classes
@@ -942,16 +945,29 @@ __global__ void k_requeue(Dev D, int count) {
 // containment proofs for drowned points (GDelPredKernels.cu:427-626)
 // --------------------------------------------------------------------------
 
-__global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_proof(Dev D, int count) {
+// EXACT = false: the FP64 filter alone; an item whose search meets an
+// undecided predicate is left untouched and its index queued on wlExact
+// (exact_next), for the exact kernel. EXACT = true: the exact predicates, over
+// the queued items (count read on the device), or over every item when the
+// queue overflowed (repeating a proof only repeats deduplicated requests).
+template <bool EXACT>
+__global__ void __launch_bounds__(32 * WARPS_PER_BLOCK, EXACT ? 1 : PROOF_BLOCKS) k_proof(Dev D, int count) {
     __shared__ int shh[WARPS_PER_BLOCK][HSLOTS];
     const int lane = threadIdx.x & 31;
     const PredSink sink = sink_of(D);
     unsigned* err = sink.err;
     unsigned* exact = &D.ctr->exact;
     const int warps = gridDim.x * WARPS_PER_BLOCK;
+    bool from_list = false;
+    if (EXACT) {
+        const int queued = *(volatile int*)&D.ctr->exact_next;
+        from_list = queued <= D.n;
+        if (from_list) count = queued;
+    }
     for (int w = blockIdx.x * WARPS_PER_BLOCK + (threadIdx.x >> 5); w < count; w += warps) {
         __syncwarp();  // the previous item's shared-memory reads are done
-        const int2 item = D.drown[w];
+        const int idx = from_list ? D.wlExact[w] : w;
+        const int2 item = D.drown[idx];
         const int s = item.x, v = item.y;
         if (!valid_id(D, s) || !valid_id(D, v)) continue;
         // a proof is needed only while v's star still links back to s
@@ -965,23 +981,30 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_proof(Dev D, int count
         const double3 pe = gpt(D, ex);
         int found_t = 0x7fffffff;
         int pa = -1, pb = -1, pc = -1;
+        bool undecided = false;
         for (int base = 0; base < h.ntri; base += 32) {
             const int t = base + lane;
-            bool ok = false;
+            bool ok = false, und = false;
             int a = -1, b = -1, c = -1;
             if (t < h.ntri) {
                 const TriU T = tri_get(V, t);
                 a = ids[T.v[0]] & (int)HID; b = ids[T.v[1]] & (int)HID; c = ids[T.v[2]] & (int)HID;
                 if (a != ex && b != ex && c != ex) {
                     const double3 qa = gpt(D, a), qb = gpt(D, b), qc = gpt(D, c);
-                    const int o0 = orient4(ps, pv, pe, qa, qb, s, v, ex, a, b, sink, exact);
-                    const int o1 = orient4(ps, pv, pe, qb, qc, s, v, ex, b, c, sink, exact);
-                    ok = o0 == o1;
+                    const int o0 = pred4<EXACT>(ps, pv, pe, qa, qb, s, v, ex, a, b, sink, exact);
+                    const int o1 = pred4<EXACT>(ps, pv, pe, qb, qc, s, v, ex, b, c, sink, exact);
+                    und = o0 == 0 || o1 == 0;
+                    ok = !und && o0 == o1;
                     if (ok) {
-                        const int o2 = orient4(ps, pv, pe, qc, qa, s, v, ex, c, a, sink, exact);
-                        ok = o1 == o2;
+                        const int o2 = pred4<EXACT>(ps, pv, pe, qc, qa, s, v, ex, c, a, sink, exact);
+                        und = o2 == 0;
+                        ok = !und && o1 == o2;
                     }
                 }
+            }
+            if (!EXACT && __any_sync(0xffffffffu, und)) {
+                undecided = true;
+                break;
             }
             const unsigned m = __ballot_sync(0xffffffffu, ok);
             if (m) {
@@ -992,6 +1015,13 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_proof(Dev D, int count
                 pc = __shfl_sync(0xffffffffu, c, src);
                 break;
             }
+        }
+        if (!EXACT && undecided) {
+            if (lane == 0) {
+                const int q = atomicAdd(&D.ctr->exact_next, 1);
+                if (q < D.n) D.wlExact[q] = w;
+            }
+            continue;
         }
         if (found_t == 0x7fffffff) {
             if (lane == 0) {
@@ -1473,8 +1503,13 @@ void launch_emit(const Launch& L, const Dev& D, int count) {
 }
 
 void launch_proof(const Launch& L, const Dev& D, int count) {
-    k_proof<<<star_blocks(count), 32 * WARPS_PER_BLOCK, 0, L.stream>>>(D, count);
-    ++*L.launches;
+    // filter-only pass, then the exact pass over what it left (its count is
+    // read on the device, so no host round trip), then the queue is emptied
+    // for the star kernels
+    k_proof<false><<<star_blocks(count), 32 * WARPS_PER_BLOCK, 0, L.stream>>>(D, count);
+    k_proof<true><<<star_blocks(count, WARPS_PER_BLOCK, 2), 32 * WARPS_PER_BLOCK, 0, L.stream>>>(D, count);
+    cudaMemsetAsync(&D.ctr->exact_next, 0, sizeof(int), L.stream);
+    *L.launches += 2;
 }
 
 void launch_check(const Launch& L, const Dev& D, unsigned long long* bad) {
