@@ -235,15 +235,15 @@ void launch_b_localize(const Launch& L, const g4d_tet* in, int ntet, const unsig
 
 // pba
 void launch_pba_z(const Launch& L, const Dev& D, uint32_t* out);
-void launch_pba_y(const Launch& L, int G, const uint32_t* in, uint32_t* out);
-void launch_pba_x(const Launch& L, int G, const uint32_t* in, uint32_t* out);
+void launch_pba_y(const Launch& L, int G, uint32_t* in, uint32_t* out);
+void launch_pba_x(const Launch& L, int G, uint32_t* in, uint32_t* out);
 void launch_pairs(const Launch& L, const Dev& D, const uint32_t* grid);
 void launch_missing(const Launch& L, const Dev& D);
 // stacks of K grids of width G (batches; 64-bit column keys)
 void launch_pba_z_stack(const Launch& L, int G, int K, const unsigned long long* ckey, const int* cs, const int* ce,
                         uint32_t* out);
-void launch_pba_y_stack(const Launch& L, int G, int K, const uint32_t* in, uint32_t* out);
-void launch_pba_x_stack(const Launch& L, int G, int K, const uint32_t* in, uint32_t* out);
+void launch_pba_y_stack(const Launch& L, int G, int K, uint32_t* in, uint32_t* out);
+void launch_pba_x_stack(const Launch& L, int G, int K, uint32_t* in, uint32_t* out);
 void launch_pairs_stack(const Launch& L, const Dev& D, const uint32_t* stack, int G, int K,
                         const unsigned long long* ckey, const int* cid, const int* cs, const int* ce);
 void launch_missing_u64(const Launch& L, const Dev& D, const unsigned long long* mkey);

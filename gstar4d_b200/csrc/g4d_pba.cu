@@ -152,6 +152,222 @@ __global__ void __launch_bounds__(256) k_pba_x(int G, const uint32_t* __restrict
 }
 
 
+// ---------------------------------------------------------------------------
+// y and x passes as lower envelopes (one thread per line, O(G) per line).
+//
+// Along a line, candidate p (a voxel whose site came from the earlier passes)
+// gives every voxel q the squared distance (q - p)^2 + f_p, f_p the squared
+// distance of its site across the line. The nearest site of each voxel is the
+// lowest of these parabolas: the lower convex hull of the points
+// (p, F_p = f_p + p^2), built in one sweep with a stack (Felzenszwalb and
+// Huttenlocher's envelope, the role of PBA's proximate-site stacks,
+// pba3DKernel.h:200-420), then read off in a second sweep. The sweep goes
+// downwards, so the stack is a list linked towards larger p; its links are
+// written into the input word of each stacked candidate (the input is
+// scratch), packed with the site coordinates the line does not fix. The
+// colouring sweep goes upwards along those links. Each thread keeps the two
+// top entries in registers, so a pop costs one load (of the new second).
+// Distances are exact; among equidistant sites the choice is free (only the
+// distance of the digital diagram is specified).
+// ---------------------------------------------------------------------------
+constexpr uint32_t ENV_END = 2047;  // end of a list (11-bit link)
+
+// Products of height differences (< 3 G^2) and position differences (< G):
+// 32-bit up to G = 512, 64-bit beyond.
+template <bool WIDE>
+using EnvInt = typename std::conditional<WIDE, long long, int>::type;
+
+// first position y at which candidate n (height fn) is at most as far as
+// candidate c (height fc), c < n: (n - c)(2y - n - c) >= fn - fc
+__device__ __forceinline__ int env_switch(int c, int fc, int n, int fn) {
+    const int A = n - c;
+    const int N = fn - fc + A * (n + c);  // switch when 2 y A >= N
+    int q = N / (2 * A);
+    if (q * 2 * A < N) ++q;
+    return q;
+}
+
+// One line of G voxels. Ops supplies: next_in(q), the input word of position
+// q (q = G-1 .. 0 in turn); put(q, w), the word left at q after pass 1 (the
+// same order); at(p), the word of an earlier position p > q (a stacked,
+// packed word); fin(w), the height of an input site; fpk(w), the height of a
+// packed word; link(w), its next position; pack(w, next); site(p, w), the
+// output site of packed word w at position p; emit(y, site) for y = 0 .. G-1
+// in turn. Pass 1 keeps the top two stack entries in registers; pass 2 moves
+// to the next envelope entry at precomputed switch positions.
+template <bool WIDE, class Ops>
+__device__ __forceinline__ void env_line(int G, Ops& o) {
+    using I = EnvInt<WIDE>;
+    int top = (int)ENV_END, sec = (int)ENV_END;
+    I Ft = 0, D = 0;  // F of the top; F_second - F_top
+    int E = 0;        // second - top
+    uint32_t wt = 0, ws = 0;
+    for (int q = G - 1; q >= 0; --q) {
+        const uint32_t w = o.next_in(q);  // q descending
+        if (w == MARKER) {
+            o.put(q, w);
+            continue;
+        }
+        const I Fq = (I)o.fin(w) + (I)q * q;
+        // pop the top while its region between q and the second is empty:
+        // (F_t - F_q)(s - t) >= (F_s - F_t)(t - q)
+        while (sec != (int)ENV_END && (Ft - Fq) * (I)E >= D * (I)(top - q)) {
+            top = sec; Ft = Ft + D; wt = ws;
+            sec = o.link(ws);
+            if (sec != (int)ENV_END) {
+                ws = o.at(sec);
+                D = (I)o.fpk(ws) + (I)sec * sec - Ft;
+                E = sec - top;
+            }
+        }
+        const uint32_t wq = o.pack(w, top);
+        o.put(q, wq);
+        sec = top; ws = wt; D = Ft - Fq; E = top - q;
+        top = q; Ft = Fq; wt = wq;
+    }
+    if (top == (int)ENV_END) {  // no site in this line
+        for (int y = 0; y < G; ++y) o.emit(y, MARKER);
+        return;
+    }
+    int cur = top, fc = o.fpk(wt), nx = o.link(wt), fn = 0, T = 1 << 30;
+    uint32_t wc = wt, wn = 0;
+    if (nx != (int)ENV_END) {
+        wn = o.at(nx);
+        fn = o.fpk(wn);
+        T = env_switch(cur, fc, nx, fn);
+    }
+    for (int y = 0; y < G; ++y) {
+        while (y >= T) {
+            cur = nx; wc = wn; fc = fn;
+            nx = o.link(wc);
+            T = 1 << 30;
+            if (nx != (int)ENV_END) {
+                wn = o.at(nx);
+                fn = o.fpk(wn);
+                T = env_switch(cur, fc, nx, fn);
+            }
+        }
+        o.emit(y, o.site(cur, wc));
+    }
+}
+
+// y pass (after the z flood): line (x, z) along y; the site of candidate p is
+// (x, p, zs), f_p = (z - zs)^2; packed word zs | next << 10. Lanes take
+// consecutive x, so every row access of a warp is one 128-byte line.
+struct EnvY {
+    uint32_t* line;
+    uint32_t* res;
+    size_t st;
+    int x, z;
+    uint32_t ahead;  // input word of the next position, loaded ahead of use
+    __device__ uint32_t next_in(int q) {
+        const uint32_t w = q == (int)(st - 1) ? line[(size_t)q * st] : ahead;
+        if (q > 0) ahead = line[(size_t)(q - 1) * st];
+        return w;
+    }
+    __device__ uint32_t at(int p) const { return line[(size_t)p * st]; }
+    __device__ void put(int p, uint32_t w) const {
+        if (w != MARKER) line[(size_t)p * st] = w;
+    }
+    __device__ int fin(uint32_t w) const { const int d = z - (int)vz(w); return d * d; }
+    __device__ int fpk(uint32_t w) const { const int d = z - (int)(w & 1023u); return d * d; }
+    __device__ int link(uint32_t w) const { return (int)((w >> 10) & 2047u); }
+    __device__ uint32_t pack(uint32_t w, int next) const { return vz(w) | ((uint32_t)next << 10); }
+    __device__ uint32_t site(int p, uint32_t w) const { return enc_vox((uint32_t)x, (uint32_t)p, w & 1023u); }
+    __device__ void emit(int y, uint32_t v) const {
+        __syncwarp();  // one full line per warp store
+        res[(size_t)y * st] = v;
+    }
+};
+
+template <bool WIDE>
+__global__ void __launch_bounds__(128) k_pba_env_y(int G, uint32_t* __restrict__ in, uint32_t* __restrict__ out) {
+    const int x = blockIdx.x * 32 + threadIdx.x;
+    const int z = blockIdx.y * 4 + threadIdx.y;
+    if (x >= G || z >= G) return;
+    const size_t plane = (size_t)G * G;
+    const size_t off = (size_t)blockIdx.z * plane * G + (size_t)z * plane + x;
+    EnvY o{in + off, out + off, (size_t)G, x, z, 0u};
+    env_line<WIDE>(G, o);
+}
+
+// x pass (after the y pass): line (y, z) along x; the site of candidate p is
+// (p, ys, zs), f_p = (y - ys)^2 + (z - zs)^2; packed word ys | zs << 10 |
+// next << 20. Lanes take consecutive y, each walking its own contiguous row,
+// so words move four at a time (16-byte accesses): pass 1 reads the next group
+// ahead, keeps the current group in registers and writes it back when it is
+// done; pass 2 writes four sites at once.
+struct EnvX {
+    uint32_t* line;
+    uint32_t* res;
+    int y, z;
+    int g0;                 // first position of the group in registers
+    uint32_t g[4];          // its words (packed once stacked)
+    uint4 ahead;            // the group below it
+    uint32_t o0, o1, o2;    // pass 2: sites of the group being emitted
+    __device__ uint32_t gsel(int d) const { return d == 0 ? g[0] : (d == 1 ? g[1] : (d == 2 ? g[2] : g[3])); }
+    __device__ uint32_t next_in(int q) {
+        if ((q & 3) == 3) {
+            const uint4 v = g0 < 0 ? *reinterpret_cast<const uint4*>(line + q - 3) : ahead;
+            g[0] = v.x; g[1] = v.y; g[2] = v.z; g[3] = v.w;
+            g0 = q - 3;
+            if (g0 > 0) ahead = *reinterpret_cast<const uint4*>(line + g0 - 4);
+        }
+        return gsel(q - g0);
+    }
+    __device__ void put(int q, uint32_t w) {
+        const int d = q - g0;
+        g[0] = d == 0 ? w : g[0];
+        g[1] = d == 1 ? w : g[1];
+        g[2] = d == 2 ? w : g[2];
+        g[3] = d == 3 ? w : g[3];
+        if (d == 0) {
+            *reinterpret_cast<uint4*>(line + g0) = make_uint4(g[0], g[1], g[2], g[3]);
+            g0 = 1 << 20;  // nothing in registers until the next group
+        }
+    }
+    __device__ uint32_t at(int p) const {
+        const int d = p - g0;
+        return (d >= 0 && d < 4) ? gsel(d) : line[p];
+    }
+    __device__ int fin(uint32_t w) const {
+        const int dy = y - (int)vy(w), dz = z - (int)vz(w);
+        return dy * dy + dz * dz;
+    }
+    __device__ int fpk(uint32_t w) const {
+        const int dy = y - (int)(w & 1023u), dz = z - (int)((w >> 10) & 1023u);
+        return dy * dy + dz * dz;
+    }
+    __device__ int link(uint32_t w) const { return (int)((w >> 20) & 2047u); }
+    __device__ uint32_t pack(uint32_t w, int next) const { return vy(w) | (vz(w) << 10) | ((uint32_t)next << 20); }
+    __device__ uint32_t site(int p, uint32_t w) const { return enc_vox((uint32_t)p, w & 1023u, (w >> 10) & 1023u); }
+    __device__ void emit(int x, uint32_t v) {
+        const int d = x & 3;
+        if (d == 0) o0 = v;
+        else if (d == 1) o1 = v;
+        else if (d == 2) o2 = v;
+        else *reinterpret_cast<uint4*>(res + x - 3) = make_uint4(o0, o1, o2, v);
+    }
+};
+
+template <bool WIDE>
+__global__ void __launch_bounds__(128) k_pba_env_x(int G, uint32_t* __restrict__ in, uint32_t* __restrict__ out) {
+    const int y = blockIdx.x * 32 + threadIdx.x;
+    const int z = blockIdx.y * 4 + threadIdx.y;
+    if (y >= G || z >= G) return;
+    const size_t plane = (size_t)G * G;
+    const size_t off = (size_t)blockIdx.z * plane * G + (size_t)z * plane + (size_t)y * G;
+    EnvX o;
+    o.line = in + off;
+    o.res = out + off;
+    o.y = y;
+    o.z = z;
+    o.g0 = -1;  // the first group is loaded directly
+    o.ahead = make_uint4(0, 0, 0, 0);
+    o.o0 = o.o1 = o.o2 = 0;
+    env_line<WIDE>(G, o);
+}
+
 #ifndef PAIR_HASH_LOG2
 #define PAIR_HASH_LOG2 11
 #endif
@@ -347,9 +563,11 @@ void launch_pba_z_stack(const Launch& L, int G, int K, const unsigned long long*
     ++*L.launches;
 }
 
-void launch_pba_y(const Launch& L, int G, const uint32_t* in, uint32_t* out) { launch_pba_y_stack(L, G, 1, in, out); }
+void launch_pba_y(const Launch& L, int G, uint32_t* in, uint32_t* out) { launch_pba_y_stack(L, G, 1, in, out); }
 
-void launch_pba_y_stack(const Launch& L, int G, int K, const uint32_t* in, uint32_t* out) {
+// `in` is scratch: the envelope passes keep their stacks in it
+void launch_pba_y_stack(const Launch& L, int G, int K, uint32_t* in, uint32_t* out) {
+#ifdef PBA_SEARCH
     // two tiles of TX*G voxels: about 34 KB for G >= 256
     const int TX = G >= 512 ? 8 : (G >= 256 ? 16 : 32);
     const size_t sm = ((size_t)TX * (G + 1) + (size_t)G * (TX + 1)) * 4;
@@ -363,12 +581,17 @@ void launch_pba_y_stack(const Launch& L, int G, int K, const uint32_t* in, uint3
 #undef G4D_Y
         default: break;
     }
+#else
+    if (G > 512) k_pba_env_y<true><<<dim3(G / 32, G / 4, K), dim3(32, 4), 0, L.stream>>>(G, in, out);
+    else k_pba_env_y<false><<<dim3(G / 32, G / 4, K), dim3(32, 4), 0, L.stream>>>(G, in, out);
+#endif
     ++*L.launches;
 }
 
-void launch_pba_x(const Launch& L, int G, const uint32_t* in, uint32_t* out) { launch_pba_x_stack(L, G, 1, in, out); }
+void launch_pba_x(const Launch& L, int G, uint32_t* in, uint32_t* out) { launch_pba_x_stack(L, G, 1, in, out); }
 
-void launch_pba_x_stack(const Launch& L, int G, int K, const uint32_t* in, uint32_t* out) {
+void launch_pba_x_stack(const Launch& L, int G, int K, uint32_t* in, uint32_t* out) {
+#ifdef PBA_SEARCH
     // TY rows of G voxels: 32 KB of shared memory per block
     const int TY = G >= 1024 ? 8 : (G >= 512 ? 16 : (G >= 256 ? 32 : (8192 / G < G ? 8192 / G : G)));
     const size_t sm = (size_t)G * TY * 4;
@@ -382,6 +605,10 @@ void launch_pba_x_stack(const Launch& L, int G, int K, const uint32_t* in, uint3
 #undef G4D_X
         default: break;
     }
+#else
+    if (G > 512) k_pba_env_x<true><<<dim3(G / 32, G / 4, K), dim3(32, 4), 0, L.stream>>>(G, in, out);
+    else k_pba_env_x<false><<<dim3(G / 32, G / 4, K), dim3(32, 4), 0, L.stream>>>(G, in, out);
+#endif
     ++*L.launches;
 }
 

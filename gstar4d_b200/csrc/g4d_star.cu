@@ -278,6 +278,33 @@ __device__ __forceinline__ int hist_state(const Dev& D, int star, int v) {
     return (e & HLINK) ? 2 : 1;
 }
 
+// hist_state(a, b) and hist_state(b, a) for valid ids, the two probe
+// sequences walked in lockstep so that their loads overlap
+__device__ __forceinline__ void hist_state_pair(const Dev& D, int a, int b, int* sab, int* sba) {
+    const StarView Va = star_view(D, a), Vb = star_view(D, b);
+    const int la = Va.large ? LargeStar::LOG2_HS : SmallStar::LOG2_HS;
+    const int lb = Vb.large ? LargeStar::LOG2_HS : SmallStar::LOG2_HS;
+    const uint32_t ma = (1u << la) - 1u, mb = (1u << lb) - 1u;
+    uint32_t pa = ((uint32_t)b * 2654435761u) >> (32 - la), pb = ((uint32_t)a * 2654435761u) >> (32 - lb);
+    int ra = -1, rb = -1;  // -1: not resolved yet
+    for (uint32_t k = 0; k <= (ma > mb ? ma : mb) && (ra < 0 || rb < 0); ++k) {
+        const uint32_t ea = ra < 0 ? (uint32_t)Va.hh[pa] : 0u;
+        const uint32_t eb = rb < 0 ? (uint32_t)Vb.hh[pb] : 0u;
+        if (ra < 0) {
+            if ((ea & HID) == (uint32_t)b) ra = (ea & HLINK) ? 2 : 1;
+            else if ((ea & HID) == HEMPTY || k == ma) ra = 0;
+            else pa = (pa + 1) & ma;
+        }
+        if (rb < 0) {
+            if ((eb & HID) == (uint32_t)a) rb = (eb & HLINK) ? 2 : 1;
+            else if ((eb & HID) == HEMPTY || k == mb) rb = 0;
+            else pb = (pb + 1) & mb;
+        }
+    }
+    *sab = ra < 0 ? 0 : ra;
+    *sba = rb < 0 ? 0 : rb;
+}
+
 __device__ __forceinline__ void push_inbox(const Dev& D, int t, int v, bool* overflow) {
     if (!valid_id(D, t) || !valid_id(D, v)) {
         atomicOr(&D.ctr->err, ERR_TOPOLOGY);
@@ -924,8 +951,10 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_emit(Dev D, int count)
                     atomicOr(&D.ctr->err, ERR_TOPOLOGY);
                     continue;
                 }
-                if (hist_state(D, a, b) == 0) push_inbox(D, a, b, &ovf);
-                if (hist_state(D, b, a) == 0) push_inbox(D, b, a, &ovf);
+                int sab, sba;
+                hist_state_pair(D, a, b, &sab, &sba);
+                if (sab == 0) push_inbox(D, a, b, &ovf);
+                if (sba == 0) push_inbox(D, b, a, &ovf);
             }
         }
         if (__ballot_sync(0xffffffffu, ovf) && lane == 0) atomicOr(&D.ctr->overflow, 1);
