@@ -94,6 +94,7 @@ struct Counters {
     int dbg_set;          // first failing exact-predicate input recorded below
     double dbg_pts[15];
     int dbg_ids[5];
+    int fix_next;         // tetra output: neighbour links written by the other side
 };
 
 __host__ __device__ inline uint32_t enc_vox(uint32_t x, uint32_t y, uint32_t z) { return x | (y << 10) | (z << 20); }
@@ -263,7 +264,9 @@ void launch_emit(const Launch& L, const Dev& D, int count);
 void launch_proof(const Launch& L, const Dev& D, int count);
 void launch_check(const Launch& L, const Dev& D, unsigned long long* bad);
 void launch_tet_count(const Launch& L, const Dev& D, int* cnt);
-void launch_tet_write(const Launch& L, const Dev& D, const int* base, g4d_tet* tets, const int* sorted_to_input);
+void launch_tet_write(const Launch& L, const Dev& D, const int* base, g4d_tet* tets, const int* sorted_to_input,
+                      int2* fix);
+void launch_tet_fix(const Launch& L, const Dev& D, g4d_tet* tets, const int2* fix);
 // learned star proposal (g4d_mlp.cu, g4d_proposal.cu)
 constexpr int MLP_NPARAMS = 9473;
 size_t mlp_infer_smem();

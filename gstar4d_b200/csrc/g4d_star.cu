@@ -1254,12 +1254,27 @@ __device__ __forceinline__ int across_t(const int* h, const typename C::Tri* gt,
     return ni;
 }
 
-// neighbour of tetrahedron (v0, v1, v2, s), s its smallest vertex, across the
-// face (v0, v1, v2), or -1. It is found through m, the smallest of v0, v1, v2:
-// the link triangle {a, s, b} of star m and the link triangle beyond its edge
-// (a, b), {a, b, y}, which is the neighbour itself (owned by m) when y > m;
-// otherwise the neighbour is owned by y.
-__device__ int face_neighbor(const Dev& D, const int* base, int s, int v0, int v1, int v2) {
+// Neighbour links between tetrahedra of different owners are resolved once,
+// by one side, which writes its own link and queues the other side's on the
+// fix list (tet id * 4 + vertex slot, value), applied by k_tet_fix:
+//  - across a face that contains the owner s, towards a neighbour owned by a
+//    smaller x: left to x (for x's tetrahedron the face is the one opposite
+//    its owner, handled below);
+//  - across the face (v0, v1, v2) opposite s: through m, the smallest of v0,
+//    v1, v2, the link triangle {a, s, b} of star m and the one beyond its
+//    edge (a, b), {a, b, y}. If y > m that triangle is the neighbour (owned by
+//    m, vertex y opposite the face); otherwise the neighbour is owned by y and
+//    the face is opposite y in it too, so the side with the smaller owner
+//    does the second lookup and writes both links.
+__device__ __forceinline__ void push_fix(const Dev& D, int2* fix, int tet, int slot, int value) {
+    const int q = atomicAdd(&D.ctr->fix_next, 1);
+    fix[q] = make_int2(tet * 4 + slot, value);
+}
+
+// link of tetrahedron `self` (vertices v0, v1, v2, s; s smallest) across the
+// face (v0, v1, v2): the neighbour's id, or -1 (no neighbour, or written later
+// through the fix list by the neighbour's owner)
+__device__ int face_neighbor(const Dev& D, const int* base, int2* fix, int self, int s, int v0, int v1, int v2) {
     const int m = min(v0, min(v1, v2));
     const int a = m == v0 ? v1 : v0, b = m == v2 ? v1 : v2;
     if (!valid_id(D, m)) return -1;
@@ -1269,14 +1284,25 @@ __device__ int face_neighbor(const Dev& D, const int* base, int s, int v0, int v
     const int ni = V.large ? across_t<LargeStar>(V.hh, static_cast<const uint4*>(V.tri), ntri, s, a, b, &y)
                            : across_t<SmallStar>(V.hh, static_cast<const uint2*>(V.tri), ntri, s, a, b, &y);
     if (ni < 0) return -1;
-    if (y > m) return kept_tet_id(D, base, m, V, ni);
-    return owned_tet_id(D, base, y, m, a, b);
+    if (y > m) {
+        const int nid = kept_tet_id(D, base, m, V, ni);
+        if (nid < 0) return -1;
+        // the neighbour's vertex slot of y
+        const TriU N = tri_get(V, ni);
+        const int j = (V.hh[N.v[0]] & (int)HID) == y ? 0 : ((V.hh[N.v[1]] & (int)HID) == y ? 1 : 2);
+        push_fix(D, fix, nid, j, self);
+        return nid;
+    }
+    if (y < s) return -1;  // y's side resolves this face
+    const int nid = owned_tet_id(D, base, y, m, a, b);
+    if (nid >= 0) push_fix(D, fix, nid, 3, self);
+    return nid;
 }
 
 // tetrahedra owned by star s (a warp)
 template <class C>
 __device__ __forceinline__ void write_star(const Dev& D, const int* base, g4d_tet* tets, const int* sorted_to_input,
-                                           int s, int ntri, const int* ids, const typename C::Tri* gt,
+                                           int2* fix, int s, int ntri, const int* ids, const typename C::Tri* gt,
                                            uint16_t* rank, int lane) {
     int pre = 0;
     for (int b0 = 0; b0 < ntri; b0 += 32) {
@@ -1302,13 +1328,10 @@ __device__ __forceinline__ void write_star(const Dev& D, const int* base, g4d_te
             for (int k = 0; k < 3; ++k)
                 if (C::tv(N, k) != e1 && C::tv(N, k) != e2) xs = C::tv(N, k);
             const int x = ids[xs] & (int)HID;
-            if (x > s)
-                out.opp[i] = C::kept(N) ? base[s] + rank[oi] : -1;
-            else
-                out.opp[i] = owned_tet_id(D, base, x, s, v[(i + 1) % 3], v[(i + 2) % 3]);
+            // a neighbour owned by x < s is linked by x's side
+            out.opp[i] = (x > s && C::kept(N)) ? base[s] + rank[oi] : -1;
         }
-        // neighbour across the face (v0, v1, v2): through star v0
-        out.opp[3] = face_neighbor(D, base, s, v[0], v[1], v[2]);
+        out.opp[3] = face_neighbor(D, base, fix, base[s] + rank[t], s, v[0], v[1], v[2]);
         if (sorted_to_input) {
             out.v[0] = sorted_to_input[v[0]];
             out.v[1] = sorted_to_input[v[1]];
@@ -1327,8 +1350,8 @@ __device__ __forceinline__ void write_star(const Dev& D, const int* base, g4d_te
 // about one remote lookup of latency instead of four), then each lane writes
 // whole tetrahedra. buf: 128 B ranks, 128 B kept list, 4 ints per kept triangle.
 __device__ __forceinline__ void write_star_small(const Dev& D, const int* base, g4d_tet* tets,
-                                                 const int* sorted_to_input, int s, int ntri, const int* ids,
-                                                 const uint2* gt, uint8_t* buf, int lane) {
+                                                 const int* sorted_to_input, int2* fix, int s, int ntri,
+                                                 const int* ids, const uint2* gt, uint8_t* buf, int lane) {
     uint8_t* rank = buf;
     uint8_t* kt = buf + 128;
     int* opp = reinterpret_cast<int*>(buf + 256);
@@ -1358,12 +1381,10 @@ __device__ __forceinline__ void write_star_small(const Dev& D, const int* base, 
             const int n0 = SmallStar::tv(N, 0), n1 = SmallStar::tv(N, 1), n2 = SmallStar::tv(N, 2);
             const int xs = (n2 != e1 && n2 != e2) ? n2 : ((n1 != e1 && n1 != e2) ? n1 : n0);
             const int x = ids[xs] & (int)HID;
-            if (x > s)
-                o = SmallStar::kept(N) ? bs + rank[oi] : -1;
-            else
-                o = owned_tet_id(D, base, x, s, f == 0 ? v1 : (f == 1 ? v2 : v0), f == 0 ? v2 : (f == 1 ? v0 : v1));
+            // a neighbour owned by x < s is linked by x's side
+            o = (x > s && SmallStar::kept(N)) ? bs + rank[oi] : -1;
         } else {
-            o = face_neighbor(D, base, s, v0, v1, v2);
+            o = face_neighbor(D, base, fix, bs + (k >> 2), s, v0, v1, v2);
         }
         opp[k] = o;
     }
@@ -1390,7 +1411,7 @@ __device__ __forceinline__ void write_star_small(const Dev& D, const int* base, 
 }
 
 __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_tet_write(Dev D, const int* base, g4d_tet* tets,
-                                                                    const int* sorted_to_input) {
+                                                                    const int* sorted_to_input, int2* fix) {
     __shared__ int shh[WARPS_PER_BLOCK][HSLOTS];
     // large stars: triangle ranks; small stars: write_star_small's buffer
     __shared__ __align__(16) uint16_t srank[WARPS_PER_BLOCK][LTSTRIDE];
@@ -1404,11 +1425,20 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_tet_write(Dev D, const
         const StarView V = star_view(D, s);
         const int* ids = stage_ids(V, shh[threadIdx.x >> 5], lane);
         if (!V.large)
-            write_star_small(D, base, tets, sorted_to_input, s, h.ntri, ids, static_cast<const uint2*>(V.tri),
+            write_star_small(D, base, tets, sorted_to_input, fix, s, h.ntri, ids, static_cast<const uint2*>(V.tri),
                              reinterpret_cast<uint8_t*>(rank), lane);
         else
-            write_star<LargeStar>(D, base, tets, sorted_to_input, s, h.ntri, ids, static_cast<const uint4*>(V.tri),
-                                  rank, lane);
+            write_star<LargeStar>(D, base, tets, sorted_to_input, fix, s, h.ntri, ids,
+                                  static_cast<const uint4*>(V.tri), rank, lane);
+    }
+}
+
+// neighbour links queued by the other side (after every record is written)
+__global__ void k_tet_fix(Dev D, g4d_tet* tets, const int2* __restrict__ fix) {
+    const int n = *(volatile int*)&D.ctr->fix_next;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int2 f = fix[i];
+        tets[f.x >> 2].opp[f.x & 3] = f.y;
     }
 }
 
@@ -1551,8 +1581,15 @@ void launch_tet_count(const Launch& L, const Dev& D, int* cnt) {
     ++*L.launches;
 }
 
-void launch_tet_write(const Launch& L, const Dev& D, const int* base, g4d_tet* tets, const int* sorted_to_input) {
-    k_tet_write<<<star_blocks(D.n), 32 * WARPS_PER_BLOCK, 0, L.stream>>>(D, base, tets, sorted_to_input);
+void launch_tet_write(const Launch& L, const Dev& D, const int* base, g4d_tet* tets, const int* sorted_to_input,
+                      int2* fix) {
+    cudaMemsetAsync(&D.ctr->fix_next, 0, sizeof(int), L.stream);
+    k_tet_write<<<star_blocks(D.n), 32 * WARPS_PER_BLOCK, 0, L.stream>>>(D, base, tets, sorted_to_input, fix);
+    ++*L.launches;
+}
+
+void launch_tet_fix(const Launch& L, const Dev& D, g4d_tet* tets, const int2* fix) {
+    k_tet_fix<<<148 * 8, 256, 0, L.stream>>>(D, tets, fix);
     ++*L.launches;
 }
 #endif  // G4D_HOST_EMULATION
