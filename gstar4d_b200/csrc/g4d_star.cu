@@ -271,38 +271,65 @@ __device__ __forceinline__ void ws_cache_coords(WS<C>& S, const Dev& D, int slot
 
 // membership of v in star `star`: 0 = never inserted, 1 = in the history but
 // not in the link, 2 = in the link
+// History probe of id v in `star`, 0 absent, 1 present, 2 linked. The first
+// probe of the small table is issued together with the class lookup (lidx), so
+// a small star, the common case, costs one round trip instead of two.
+struct HistProbe {
+    const int* h;
+    uint32_t mask, pos, e;
+    int r;  // -1 while unresolved
+};
+
+__device__ __forceinline__ HistProbe hist_begin(const Dev& D, int star, int v) {
+    const int li = D.anyLarge ? D.lidx[star] : -1;
+    const uint32_t q = hslot0<SmallStar::LOG2_HS>(v);
+    const uint32_t e0 = (uint32_t)D.hh[(size_t)star * HSLOTS + q];
+    HistProbe P;
+    P.r = -1;
+    if (li < 0) {
+        P.h = D.hh + (size_t)star * HSLOTS;
+        P.mask = HSLOTS - 1;
+        P.pos = q;
+        P.e = e0;
+    } else {
+        P.h = D.lhh + (size_t)li * LHSLOTS;
+        P.mask = LHSLOTS - 1;
+        P.pos = hslot0<LargeStar::LOG2_HS>(v);
+        P.e = (uint32_t)P.h[P.pos];
+    }
+    return P;
+}
+
+// resolve with the current entry (probe k) or move to the next slot
+__device__ __forceinline__ void hist_step(HistProbe& P, int v, uint32_t k) {
+    if ((P.e & HID) == (uint32_t)v) P.r = (P.e & HLINK) ? 2 : 1;
+    else if ((P.e & HID) == HEMPTY || k == P.mask) P.r = 0;
+    else P.pos = (P.pos + 1) & P.mask;
+}
+
 __device__ __forceinline__ int hist_state(const Dev& D, int star, int v) {
     if (!valid_id(D, star)) return 1;  // never asks for an insertion into a bad star
-    uint32_t e = 0;
-    if (view_lookup(star_view(D, star), v, &e) < 0) return 0;
-    return (e & HLINK) ? 2 : 1;
+    HistProbe P = hist_begin(D, star, v);
+    for (uint32_t k = 0;; ++k) {
+        hist_step(P, v, k);
+        if (P.r >= 0) return P.r;
+        P.e = (uint32_t)P.h[P.pos];
+    }
 }
 
 // hist_state(a, b) and hist_state(b, a) for valid ids, the two probe
 // sequences walked in lockstep so that their loads overlap
 __device__ __forceinline__ void hist_state_pair(const Dev& D, int a, int b, int* sab, int* sba) {
-    const StarView Va = star_view(D, a), Vb = star_view(D, b);
-    const int la = Va.large ? LargeStar::LOG2_HS : SmallStar::LOG2_HS;
-    const int lb = Vb.large ? LargeStar::LOG2_HS : SmallStar::LOG2_HS;
-    const uint32_t ma = (1u << la) - 1u, mb = (1u << lb) - 1u;
-    uint32_t pa = ((uint32_t)b * 2654435761u) >> (32 - la), pb = ((uint32_t)a * 2654435761u) >> (32 - lb);
-    int ra = -1, rb = -1;  // -1: not resolved yet
-    for (uint32_t k = 0; k <= (ma > mb ? ma : mb) && (ra < 0 || rb < 0); ++k) {
-        const uint32_t ea = ra < 0 ? (uint32_t)Va.hh[pa] : 0u;
-        const uint32_t eb = rb < 0 ? (uint32_t)Vb.hh[pb] : 0u;
-        if (ra < 0) {
-            if ((ea & HID) == (uint32_t)b) ra = (ea & HLINK) ? 2 : 1;
-            else if ((ea & HID) == HEMPTY || k == ma) ra = 0;
-            else pa = (pa + 1) & ma;
-        }
-        if (rb < 0) {
-            if ((eb & HID) == (uint32_t)a) rb = (eb & HLINK) ? 2 : 1;
-            else if ((eb & HID) == HEMPTY || k == mb) rb = 0;
-            else pb = (pb + 1) & mb;
-        }
+    HistProbe A = hist_begin(D, a, b), B = hist_begin(D, b, a);
+    for (uint32_t k = 0;; ++k) {
+        if (A.r < 0) hist_step(A, b, k);
+        if (B.r < 0) hist_step(B, a, k);
+        if (A.r >= 0 && B.r >= 0) break;
+        if (A.r < 0) A.e = (uint32_t)A.h[A.pos];
+        if (B.r < 0) B.e = (uint32_t)B.h[B.pos];
     }
-    *sab = ra < 0 ? 0 : ra;
-    *sba = rb < 0 ? 0 : rb;
+    *sab = A.r;
+    *sba = B.r;
 }
 
 __device__ __forceinline__ void push_inbox(const Dev& D, int t, int v, bool* overflow) {
@@ -1096,10 +1123,8 @@ __device__ __forceinline__ int hash_slot(const int* h, int v) {
 // index of the triangle with vertex ids {x,y,z} (cyclic x,y,z when `cyclic`)
 // in a class-C star, or -1
 template <class C>
-__device__ __forceinline__ int find_tri_t(const int* h, const typename C::Tri* gt, int ntri, int x, int y, int z,
-                                          bool cyclic) {
-    const int sx = hash_slot<C>(h, x), sy = hash_slot<C>(h, y), sz = hash_slot<C>(h, z);
-    if (sx < 0 || sy < 0 || sz < 0) return -1;
+__device__ __forceinline__ int find_tri_slots(const typename C::Tri* gt, int ntri, int sx, int sy, int sz,
+                                              bool cyclic) {
     // four triangles per step, loaded together (clamped to the last one)
     for (int t0 = 0; t0 < ntri; t0 += 4) {
         typename C::Tri T[4];
@@ -1120,6 +1145,52 @@ __device__ __forceinline__ int find_tri_t(const int* h, const typename C::Tri* g
         }
     }
     return -1;
+}
+
+template <class C>
+__device__ __forceinline__ int find_tri_t(const int* h, const typename C::Tri* gt, int ntri, int x, int y, int z,
+                                          bool cyclic) {
+    const int sx = hash_slot<C>(h, x), sy = hash_slot<C>(h, y), sz = hash_slot<C>(h, z);
+    if (sx < 0 || sy < 0 || sz < 0) return -1;
+    return find_tri_slots<C>(gt, ntri, sx, sy, sz, cyclic);
+}
+
+// small-table slot of v given the entry at its first probe position
+__device__ __forceinline__ int hash_slot_small(const int* h, int v, uint32_t e) {
+    uint32_t s = hslot0<SmallStar::LOG2_HS>(v);
+    for (int k = 0;; ++k) {
+        if ((e & HID) == (uint32_t)v) return (int)s;
+        if ((e & HID) == HEMPTY || k == SmallStar::HS - 1) return -1;
+        s = (s + 1) & (SmallStar::HS - 1);
+        e = (uint32_t)h[s];
+    }
+}
+
+// triangle of `star` with vertex ids {x, y, z} in any order (and its view),
+// or -1. The first probes of the small table are issued together with the
+// class and size lookups, so a small star's lookup starts one round trip
+// earlier.
+__device__ __forceinline__ int find_tri_spec(const Dev& D, int star, int x, int y, int z, StarView* Vout) {
+    const int li = D.anyLarge ? D.lidx[star] : -1;
+    const int* hs = D.hh + (size_t)star * HSLOTS;
+    const uint32_t ex = (uint32_t)hs[hslot0<SmallStar::LOG2_HS>(x)];
+    const uint32_t ey = (uint32_t)hs[hslot0<SmallStar::LOG2_HS>(y)];
+    const uint32_t ez = (uint32_t)hs[hslot0<SmallStar::LOG2_HS>(z)];
+    const int ntri = D.hdr[star].ntri;
+    StarView V;
+    V.large = li >= 0;
+    if (V.large) {
+        V.hh = D.lhh + (size_t)li * LHSLOTS;
+        V.tri = D.ltri + (size_t)li * LTSTRIDE;
+        *Vout = V;
+        return find_tri_t<LargeStar>(V.hh, static_cast<const uint4*>(V.tri), ntri, x, y, z, false);
+    }
+    V.hh = hs;
+    V.tri = D.tri + (size_t)star * TSTRIDE;
+    *Vout = V;
+    const int sx = hash_slot_small(hs, x, ex), sy = hash_slot_small(hs, y, ey), sz = hash_slot_small(hs, z, ez);
+    if (sx < 0 || sy < 0 || sz < 0) return -1;
+    return find_tri_slots<SmallStar>(static_cast<const uint2*>(V.tri), ntri, sx, sy, sz, false);
 }
 
 __device__ int find_tri(const Dev& D, int star, int x, int y, int z, bool cyclic) {
@@ -1210,40 +1281,15 @@ __device__ __forceinline__ int kept_tet_id(const Dev& D, const int* base, int st
 // other vertices are {x,y,z}, or -1
 __device__ int owned_tet_id(const Dev& D, const int* base, int star, int x, int y, int z) {
     if (!valid_id(D, star)) return -1;
-    const StarView V = star_view(D, star);
-    const int ntri = D.hdr[star].ntri;
-    const int ti = V.large ? find_tri_t<LargeStar>(V.hh, static_cast<const uint4*>(V.tri), ntri, x, y, z, false)
-                           : find_tri_t<SmallStar>(V.hh, static_cast<const uint2*>(V.tri), ntri, x, y, z, false);
+    StarView V;
+    const int ti = find_tri_spec(D, star, x, y, z, &V);
     return ti < 0 ? -1 : kept_tet_id(D, base, star, V, ti);
 }
 
-// the vertex y beyond edge (b,c) from s in star a: the triangle (b, s, c) of
-// star a and its neighbour across (b, c) = (b, c, y); -1 if absent
+// star m's link triangle ta and the triangle beyond its edge opposite vertex
+// id s: returns that triangle's index and sets *y to its vertex not in {a, b}
 template <class C>
-__device__ __forceinline__ int across_t(const int* h, const typename C::Tri* gt, int ntri, int s, int b, int c) {
-    const int ta = find_tri_t<C>(h, gt, ntri, b, s, c, false);
-    if (ta < 0) return -1;
-    const typename C::Tri A = gt[ta];
-    int pos = 0;
-    for (int k = 0; k < 3; ++k)
-        if ((h[C::tv(A, k)] & (int)HID) == s) pos = k;
-    const typename C::Tri N = gt[C::to(A, pos)];
-    int y = -1;
-    for (int k = 0; k < 3; ++k) {
-        const int id = h[C::tv(N, k)] & (int)HID;
-        if (id != b && id != c) y = id;
-    }
-    return y;
-}
-
-// star m's triangle {a, s, b} and the triangle beyond its edge (a, b): returns
-// the index of that neighbour triangle and sets *y to its third vertex; -1 if
-// absent
-template <class C>
-__device__ __forceinline__ int across_t(const int* h, const typename C::Tri* gt, int ntri, int s, int a, int b,
-                                        int* y) {
-    const int ta = find_tri_t<C>(h, gt, ntri, a, s, b, false);
-    if (ta < 0) return -1;
+__device__ __forceinline__ int across_t(const int* h, const typename C::Tri* gt, int ta, int s, int a, int b, int* y) {
     const typename C::Tri A = gt[ta];
     const int i0 = h[C::tv(A, 0)] & (int)HID, i1 = h[C::tv(A, 1)] & (int)HID;
     const int pos = i0 == s ? 0 : (i1 == s ? 1 : 2);
@@ -1278,12 +1324,12 @@ __device__ int face_neighbor(const Dev& D, const int* base, int2* fix, int self,
     const int m = min(v0, min(v1, v2));
     const int a = m == v0 ? v1 : v0, b = m == v2 ? v1 : v2;
     if (!valid_id(D, m)) return -1;
-    const StarView V = star_view(D, m);
-    const int ntri = D.hdr[m].ntri;
+    StarView V;
+    const int ta = find_tri_spec(D, m, a, s, b, &V);
+    if (ta < 0) return -1;
     int y = -1;
-    const int ni = V.large ? across_t<LargeStar>(V.hh, static_cast<const uint4*>(V.tri), ntri, s, a, b, &y)
-                           : across_t<SmallStar>(V.hh, static_cast<const uint2*>(V.tri), ntri, s, a, b, &y);
-    if (ni < 0) return -1;
+    const int ni = V.large ? across_t<LargeStar>(V.hh, static_cast<const uint4*>(V.tri), ta, s, a, b, &y)
+                           : across_t<SmallStar>(V.hh, static_cast<const uint2*>(V.tri), ta, s, a, b, &y);
     if (y > m) {
         const int nid = kept_tet_id(D, base, m, V, ni);
         if (nid < 0) return -1;
