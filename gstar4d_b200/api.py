@@ -61,7 +61,7 @@ _lib = None
 EXPORTS = ["g4d_default_config", "g4d_create", "g4d_destroy", "g4d_last_error", "g4d_status_string",
            "g4d_triangulate", "g4d_triangulate_to", "g4d_triangulate_device", "g4d_gdel_init",
            "g4d_gdel_compute", "g4d_get_tetra", "g4d_gdel_deinit", "g4d_get_stats", "g4d_triangulate_batch",
-           "g4d_triangulate_batch_device", "g4d_stream",
+           "g4d_triangulate_batch_to", "g4d_triangulate_batch_device", "g4d_stream",
            "g4d_eval_predicates", "g4d_voronoi", "g4d_voronoi_noalloc", "g4d_proposal_train",
            "g4d_proposal_weights", "g4d_mlp_grad", "g4d_mlp_infer", "g4d_free"]
 
@@ -94,6 +94,8 @@ def load():
     L.g4d_get_stats.argtypes = [vp, ctypes.POINTER(Stats)]
     L.g4d_triangulate_batch.argtypes = [vp, vp, vp, ip, ctypes.POINTER(vp), ctypes.POINTER(vp),
                                         ctypes.POINTER(Stats)]
+    L.g4d_triangulate_batch_to.argtypes = [vp, vp, vp, ip, vp, ctypes.c_int64, vp, ctypes.POINTER(ctypes.c_int64),
+                                           ctypes.POINTER(Stats)]
     L.g4d_triangulate_batch_device.argtypes = [vp, vp, vp, ip, ctypes.POINTER(vp), ctypes.POINTER(vp),
                                                ctypes.POINTER(Stats)]
     L.g4d_eval_predicates.argtypes = [vp, ip, vp, vp, ip, vp]
@@ -289,12 +291,27 @@ class Triangulator:
     def gdel_deinit(self):
         self._check(self._lib.g4d_gdel_deinit(self._h))
 
-    def triangulate_batch(self, points, cloud_offsets):
+    def triangulate_batch(self, points, cloud_offsets, out=None):
+        """Tetrahedra of many clouds: (tets, tet_offsets, stats), cloud c's
+        tetrahedra are tets[tet_offsets[c]:tet_offsets[c+1]] with cloud-local
+        input indices. With `out` (a TET_DTYPE array, best in pinned memory) the
+        results are copied into it while later passes compute and tets is a
+        view of it."""
         pts = np.ascontiguousarray(points, dtype=np.float64)
         offs = np.ascontiguousarray(cloud_offsets, dtype=np.int64)
-        tp, op = ctypes.c_void_p(), ctypes.c_void_p()
         stats = Stats()
         nclouds = len(offs) - 1
+        if out is not None:
+            if out.dtype != TET_DTYPE or not out.flags.c_contiguous:
+                raise ValueError("out must be a contiguous TET_DTYPE array")
+            toffs = np.zeros(nclouds + 1, np.int64)
+            nt = ctypes.c_int64()
+            st = self._lib.g4d_triangulate_batch_to(self._h, _ptr(pts), _ptr(offs), nclouds, _ptr(out), len(out),
+                                                    _ptr(toffs), ctypes.byref(nt), ctypes.byref(stats))
+            self._check(st)
+            self.last_stats = stats.as_dict()
+            return out[: nt.value], toffs, self.last_stats
+        tp, op = ctypes.c_void_p(), ctypes.c_void_p()
         st = self._lib.g4d_triangulate_batch(self._h, _ptr(pts), _ptr(offs), nclouds, ctypes.byref(tp),
                                              ctypes.byref(op), ctypes.byref(stats))
         self._check(st)

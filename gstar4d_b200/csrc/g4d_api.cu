@@ -63,6 +63,7 @@ struct g4d_ctx {
     g4d_config cfg;
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t copy_stream = nullptr;  // batch results to host while the next pass computes
     Buf b[B_NUM];
     std::string err;
     // results of the last compute
@@ -663,6 +664,7 @@ g4d_status reserve_out(g4d_ctx* ctx, size_t used, size_t need) {
     CK(cudaMalloc(&np, want));
     if (used && o.p) CK(cudaMemcpyAsync(np, o.p, used * sizeof(g4d_tet), cudaMemcpyDeviceToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    if (ctx->copy_stream) CK(cudaStreamSynchronize(ctx->copy_stream));  // host copies out of the old buffer
     o.release();
     o.p = np;
     o.cap = want;
@@ -946,8 +948,16 @@ g4d_status pick_batch_grids(g4d_ctx* ctx, const double* d_xyz, const int64_t* of
 
 // All waves of a batch whose points are on the device; the tetrahedra end in
 // B_BOUT (cloud order) and counts[c] per cloud.
+// Optional host destination of a batch: each pass's tetrahedra are copied on
+// the copy stream while the next pass computes (as long as they fit in cap).
+struct HostSink {
+    g4d_tet* out;
+    size_t cap;
+    bool fits;
+};
+
 g4d_status run_batch(g4d_ctx* ctx, const double* d_xyz, const int64_t* offs, int nclouds,
-                     std::vector<int64_t>& counts, size_t* total, g4d_stats* acc) {
+                     std::vector<int64_t>& counts, size_t* total, g4d_stats* acc, HostSink* sink = nullptr) {
     for (int c = 0; c < nclouds; ++c) {
         const int64_t n = offs[c + 1] - offs[c];
         if (n < 5 || n >= (1 << 30))
@@ -969,13 +979,19 @@ g4d_status run_batch(g4d_ctx* ctx, const double* d_xyz, const int64_t* offs, int
     size_t at = 0;
     int large = 0;
     std::vector<int> list;
+    // G4D_WAVE_POINTS lowers the points per pass (tests use it to get many passes)
+    long long wave_points = kWavePoints;
+    if (const char* e = getenv("G4D_WAVE_POINTS")) {
+        const long long v = atoll(e);
+        if (v > 0 && v < kWavePoints) wave_points = v;
+    }
     for (int c0 = 0; c0 < nclouds;) {
         int c1 = c0;
         long long pts = 0, vox = 0;
         while (c1 < nclouds) {
             const long long n = offs[c1 + 1] - offs[c1];
             const long long v = (long long)Gc[c1] * Gc[c1] * Gc[c1];
-            if (c1 > c0 && (pts + n > kWavePoints || vox + v > kWaveVoxels)) break;
+            if (c1 > c0 && (pts + n > wave_points || vox + v > kWaveVoxels)) break;
             pts += n;
             vox += v;
             ++c1;
@@ -985,6 +1001,16 @@ g4d_status run_batch(g4d_ctx* ctx, const double* d_xyz, const int64_t* offs, int
         size_t wt = 0;
         st = run_wave(ctx, d_xyz, offs, list.data(), c1 - c0, Gc.data(), at, counts.data(), &wt);
         if (st) return st;
+        if (sink && sink->fits) {
+            if (at + wt <= sink->cap) {
+                CK(cudaEventRecord(ctx->ev[7], ctx->stream));
+                CK(cudaStreamWaitEvent(ctx->copy_stream, ctx->ev[7], 0));
+                CK(cudaMemcpyAsync(sink->out + at, ctx->b[B_BOUT].as<g4d_tet>() + at, sizeof(g4d_tet) * wt,
+                                   cudaMemcpyDeviceToHost, ctx->copy_stream));
+            } else {
+                sink->fits = false;
+            }
+        }
         at += wt;
         acc->t_init_ms += ms_between(ctx->ev[0], ctx->ev[1]);
         acc->t_pba_ms += ms_between(ctx->ev[1], ctx->ev[2]);
@@ -1069,6 +1095,11 @@ g4d_status g4d_create(g4d_ctx** out, const g4d_config* cfg) {
         delete ctx;
         return G4D_ERR_CUDA;
     }
+    if (cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaStreamDestroy(ctx->stream);
+        delete ctx;
+        return G4D_ERR_CUDA;
+    }
     for (auto& e : ctx->ev) cudaEventCreate(&e);
     *out = ctx;
     return G4D_OK;
@@ -1078,8 +1109,10 @@ void g4d_destroy(g4d_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
     for (auto& b : ctx->b) b.release();
     for (auto& e : ctx->ev) cudaEventDestroy(e);
+    if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -1267,6 +1300,35 @@ g4d_status g4d_triangulate_batch(g4d_ctx* ctx, const double* xyz, const int64_t*
     CK(cudaStreamSynchronize(ctx->stream));
     *tets = out;
     *tet_offsets = offs;
+    acc.t_total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    ctx->stats = acc;
+    if (stats) *stats = acc;
+    return G4D_OK;
+}
+
+g4d_status g4d_triangulate_batch_to(g4d_ctx* ctx, const double* xyz, const int64_t* cloud_offsets, int nclouds,
+                                    g4d_tet* out, int64_t cap, int64_t* tet_offsets, int64_t* ntet,
+                                    g4d_stats* stats) {
+    if (!ctx) return G4D_ERR_ARG;
+    if (!xyz || !cloud_offsets || nclouds < 0 || !out || cap < 0 || !tet_offsets || !ntet)
+        return fail(ctx, G4D_ERR_ARG, "null argument");
+    *ntet = 0;
+    cudaSetDevice(ctx->device);
+    const auto t0 = std::chrono::steady_clock::now();
+    const int64_t total = nclouds ? cloud_offsets[nclouds] : 0;
+    CK(ctx->b[B_XYZ].ensure(sizeof(double) * 3 * (size_t)std::max<int64_t>(total, 1)));
+    CK(cudaMemcpyAsync(ctx->b[B_XYZ].p, xyz, sizeof(double) * 3 * (size_t)total, cudaMemcpyHostToDevice, ctx->stream));
+    std::vector<int64_t> counts;
+    size_t nt = 0;
+    g4d_stats acc{};
+    HostSink sink{out, (size_t)cap, true};
+    g4d_status st = run_batch(ctx, ctx->b[B_XYZ].as<double>(), cloud_offsets, nclouds, counts, &nt, &acc, &sink);
+    CK(cudaStreamSynchronize(ctx->copy_stream));
+    if (st) return st;
+    tet_offsets[0] = 0;
+    for (int c = 0; c < nclouds; ++c) tet_offsets[c + 1] = tet_offsets[c] + counts[c];
+    *ntet = (int64_t)nt;
+    if (!sink.fits) return fail(ctx, G4D_ERR_ARG, "output buffer too small (%lld < %zu)", (long long)cap, nt);
     acc.t_total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     ctx->stats = acc;
     if (stats) *stats = acc;

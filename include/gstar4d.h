@@ -151,6 +151,15 @@ G4D_API g4d_status g4d_get_stats(const g4d_ctx* ctx, g4d_stats* stats);
 G4D_API g4d_status g4d_triangulate_batch(g4d_ctx* ctx, const double* xyz, const int64_t* cloud_offsets, int nclouds,
                                  g4d_tet** tets, int64_t** tet_offsets, g4d_stats* stats);
 
+/* The same into a caller buffer `out` of `cap` tetrahedra (pinned host memory
+ * makes the copies run at full speed): each pass's tetrahedra are copied while
+ * the next pass computes. tet_offsets (nclouds + 1 entries) and *ntet are set
+ * in any case; when the batch has more than cap tetrahedra the call returns
+ * G4D_ERR_ARG and out is incomplete. */
+G4D_API g4d_status g4d_triangulate_batch_to(g4d_ctx* ctx, const double* xyz, const int64_t* cloud_offsets,
+                                            int nclouds, g4d_tet* out, int64_t cap, int64_t* tet_offsets,
+                                            int64_t* ntet, g4d_stats* stats);
+
 /* The same with the points already on ctx's device (d_xyz, 3 doubles per
  * point); cloud_offsets stays on the host. The tetrahedra stay in a
  * context-owned device buffer (*d_tets) and *tet_offsets points to

@@ -105,3 +105,28 @@ def test_batch_rejects_tiny_cloud():
         with pytest.raises(gstar4d_b200.G4DError) as e:
             t.triangulate_batch(pts, np.array([0, 3, 20], np.int64))
     assert e.value.status == 1
+
+
+def test_batch_into_pinned_buffer_over_many_passes(oracle, monkeypatch):
+    """g4d_triangulate_batch_to: results copied into a caller (pinned) buffer
+    pass by pass while later passes compute; passes limited to 20k points so
+    the batch takes several. Every cloud must match the library-allocated
+    batch; a buffer one tetrahedron short is refused with the count set."""
+    import torch
+    import gstar4d_b200
+    monkeypatch.setenv("G4D_WAVE_POINTS", "20000")
+    clouds, pts, offs = _batch(30, seed=8, hi=9000)
+    with gstar4d_b200.Triangulator(grid_size=64) as t:
+        ref, ref_offs, _ = t.triangulate_batch(pts, offs)
+        buf = torch.empty((len(ref) + 16, 8), dtype=torch.int32).pin_memory()
+        out = buf.numpy().view(gstar4d_b200.TET_DTYPE).reshape(-1)
+        got, got_offs, _ = t.triangulate_batch(pts, offs, out=out)
+        assert np.array_equal(got_offs, ref_offs) and len(got) == len(ref)
+        for c in range(len(clouds)):
+            a = _canon(oracle, got[got_offs[c]:got_offs[c + 1]])
+            b = _canon(oracle, ref[ref_offs[c]:ref_offs[c + 1]])
+            assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]), c
+        short = out[: len(ref) - 1]
+        with pytest.raises(gstar4d_b200.G4DError) as e:
+            t.triangulate_batch(pts, offs, out=short)
+        assert e.value.status == 1
