@@ -970,19 +970,52 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_emit(Dev D, int count)
         for (int t = lane; t < h.ntri; t += 32) {
             const TriU T = tri_get(V, t);
             if (T.gen != h.pass) continue;
-            const int v[3] = {ids[T.v[0]] & (int)HID, ids[T.v[1]] & (int)HID, ids[T.v[2]] & (int)HID};
+            const int v0 = ids[T.v[0]] & (int)HID, v1 = ids[T.v[1]] & (int)HID, v2 = ids[T.v[2]] & (int)HID;
+            // edges (v0,v1), (v1,v2), (v2,v0), each taken from the triangle
+            // that lists it in increasing order
+            const int ea[3] = {v0, v1, v2}, eb[3] = {v1, v2, v0};
+            bool need[3];
+#pragma unroll
             for (int i = 0; i < 3; ++i) {
-                const int a = v[i], b = v[(i + 1) % 3];
-                if (a > b) continue;
-                if (!valid_id(D, a) || !valid_id(D, b)) {
+                need[i] = ea[i] < eb[i];
+                if (need[i] && (!valid_id(D, ea[i]) || !valid_id(D, eb[i]))) {
                     atomicOr(&D.ctr->err, ERR_TOPOLOGY);
-                    continue;
+                    need[i] = false;
                 }
-                int sab, sba;
-                hist_state_pair(D, a, b, &sab, &sba);
-                if (sab == 0) push_inbox(D, a, b, &ovf);
-                if (sba == 0) push_inbox(D, b, a, &ovf);
             }
+            // Histories stay symmetric up to pending requests: every id
+            // entered a's history through the initial workset (built from
+            // symmetric pairs) or through a request (a <- b), and every place
+            // that queues (a <- b) also checks and queues (b <- a) (overflowing
+            // requests are re-sent). So b in a's history means a is in b's or
+            // on its way, and only when b is missing from a's history does the
+            // other direction need a lookup. The three edges' probes go out
+            // together.
+            HistProbe P[3];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                P[i].r = 1;
+                if (need[i]) P[i] = hist_begin(D, ea[i], eb[i]);
+            }
+            for (uint32_t k = 0;; ++k) {
+                bool open = false;
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+                    if (P[i].r < 0) {
+                        hist_step(P[i], eb[i], k);
+                        open |= P[i].r < 0;
+                    }
+                if (!open) break;
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+                    if (P[i].r < 0) P[i].e = (uint32_t)P[i].h[P[i].pos];
+            }
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+                if (need[i] && P[i].r == 0) {
+                    push_inbox(D, ea[i], eb[i], &ovf);
+                    if (hist_state(D, eb[i], ea[i]) == 0) push_inbox(D, eb[i], ea[i], &ovf);
+                }
         }
         if (__ballot_sync(0xffffffffu, ovf) && lane == 0) atomicOr(&D.ctr->overflow, 1);
     }
