@@ -624,8 +624,11 @@ __device__ void warp_load(WS<C>& S, const Dev& D, int lane, int s, StarHdr h) {
 }
 
 // Compact triangles, refresh link bits, report drowned points, write back.
+// full: the whole history table (a star built here); otherwise only the slots
+// that changed (new ids, link bits that flipped), and the triangles only when
+// `created` (they changed).
 template <class C>
-__device__ void warp_store(WS<C>& S, const Dev& D, int lane, int s, int pass, bool created) {
+__device__ void warp_store(WS<C>& S, const Dev& D, int lane, int s, int pass, bool created, bool full) {
     using Idx = typename C::Idx;
     const int ntri = S.ntri;
     int nalive = 0;
@@ -645,7 +648,7 @@ __device__ void warp_store(WS<C>& S, const Dev& D, int lane, int s, int pass, bo
     }
     __syncwarp();
     typename C::Tri* gt = C::tris(D, s);
-    for (int t = lane; t < ntri; t += 32) {
+    for (int t = lane; t < ntri && (created || full); t += 32) {
         if (!(S.tf[t] & 0x80)) continue;
         gt[S.blist[t]] = C::pack(S.tv[0][t], S.tv[1][t], S.tv[2][t], S.tf[t] & 15, S.blist[S.to[0][t]],
                                  S.blist[S.to[1][t]], S.blist[S.to[2][t]], S.tj[0][t], S.tj[1][t], S.tj[2][t]);
@@ -654,9 +657,10 @@ __device__ void warp_store(WS<C>& S, const Dev& D, int lane, int s, int pass, bo
     int* gh = C::hash(D, s);
     for (int k = lane; k < C::HS; k += 32) {
         const int e = S.hh[k];
-        gh[k] = e;
+        const bool was = (S.wasLink[k >> 5] >> (k & 31)) & 1u, ins = (S.insMask[k >> 5] >> (k & 31)) & 1u;
+        if (full || ins || was != ((e & (int)HLINK) != 0)) gh[k] = e;
         const bool occupied = (uint32_t)(e & (int)HID) != HEMPTY;
-        const bool before = ((S.wasLink[k >> 5] | S.insMask[k >> 5]) >> (k & 31)) & 1u;
+        const bool before = was || ins;
         const bool dr = occupied && before && !(e & (int)HLINK);
         const unsigned m = __ballot_sync(0xffffffffu, dr);
         if (m) {
@@ -811,7 +815,7 @@ __global__ void __launch_bounds__(32 * C::WARPS, EXACT ? C::MINB : C::MINB_FAST)
                 continue;
             }
         }
-        warp_store(S, D, lane, s, gen, true);
+        warp_store(S, D, lane, s, gen, true, true);
         if (lane == 0) atomicAdd(&D.ctr->insertions, (unsigned long long)nins);
     }
 }
@@ -889,7 +893,7 @@ __global__ void __launch_bounds__(32 * C::WARPS, EXACT ? C::MINB : C::MINB_FAST)
         if (failed) continue;
         for (int k = lane; k < ic; k += 32) box[k] = -1;  // the inbox is consumed
         if (lane == 0) D.inboxCount[s] = 0;
-        warp_store(S, D, lane, s, any ? gen : h.pass, any != 0);
+        warp_store(S, D, lane, s, any ? gen : h.pass, any != 0, false);
         if (lane == 0) atomicAdd(&D.ctr->insertions, (unsigned long long)nins);
     }
 }
