@@ -1264,30 +1264,61 @@ __global__ void k_check(Dev D, unsigned long long* bad) {
 // so that any star's rank is a few popcounts.
 // --------------------------------------------------------------------------
 
-__global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_tet_count(Dev D, int* cnt) {
+// EXACT = false: the orient3d filter alone; a star with an undecided triangle
+// is left untouched and queued on wlExact for the exact kernel, which takes
+// its count from the device (or every star when the queue overflowed).
+template <bool EXACT>
+__global__ void __launch_bounds__(32 * WARPS_PER_BLOCK, EXACT ? 1 : 8) k_tet_count(Dev D, int* cnt) {
     __shared__ int shh[WARPS_PER_BLOCK][HSLOTS];
     const int lane = threadIdx.x & 31;
     const PredSink sink = sink_of(D);
     const int warps = gridDim.x * WARPS_PER_BLOCK;
-    for (int s = blockIdx.x * WARPS_PER_BLOCK + (threadIdx.x >> 5); s < D.n; s += warps) {
+    int count = D.n;
+    bool from_list = false;
+    if (EXACT) {
+        const int queued = *(volatile int*)&D.ctr->exact_next;
+        from_list = queued <= D.n;
+        if (from_list) count = queued;
+    }
+    for (int w = blockIdx.x * WARPS_PER_BLOCK + (threadIdx.x >> 5); w < count; w += warps) {
+        const int s = from_list ? D.wlExact[w] : w;
         __syncwarp();  // the previous star's shared-memory reads are done
         const StarHdr h = D.hdr[s];
         const StarView V = star_view(D, s);
         const int* ids = stage_ids(V, shh[threadIdx.x >> 5], lane);
         const double3 ps = gpt(D, s);
+        // (an undecided sign leaves the star to the exact kernel, which
+        // rewrites every kept bit and the count)
         int c = 0;
+        bool undecided = false;
         for (int b0 = 0; b0 < h.ntri; b0 += 32) {
             const int t = b0 + lane;
-            bool keep = false;
+            bool keep = false, und = false;
             if (t < h.ntri) {
                 const TriU T = tri_get(V, t);
                 const int a = ids[T.v[0]] & (int)HID, b = ids[T.v[1]] & (int)HID, cc = ids[T.v[2]] & (int)HID;
-                if (s < a && s < b && s < cc) keep = orient3d(gpt(D, a), gpt(D, b), gpt(D, cc), ps, sink) < 0;
+                if (s < a && s < b && s < cc) {
+                    const int sg = EXACT ? orient3d(gpt(D, a), gpt(D, b), gpt(D, cc), ps, sink)
+                                         : orient3d_filter(gpt(D, a), gpt(D, b), gpt(D, cc), ps);
+                    keep = sg < 0;
+                    und = sg == 0;
+                }
                 tri_set_kept(V, t, keep);
+            }
+            if (!EXACT && __any_sync(0xffffffffu, und)) {
+                undecided = true;
+                break;
             }
             const unsigned m = __ballot_sync(0xffffffffu, keep);
             if (!V.large && lane == 0) D.keptMask[(size_t)s * (TSTRIDE / 32) + (b0 >> 5)] = m;
             c += keep;
+        }
+        if (undecided) {
+            if (lane == 0) {
+                const int q = atomicAdd(&D.ctr->exact_next, 1);
+                if (q < D.n) D.wlExact[q] = s;
+            }
+            continue;
         }
         for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
         if (lane == 0) cnt[s] = c;
@@ -1660,8 +1691,13 @@ void launch_check(const Launch& L, const Dev& D, unsigned long long* bad) {
 }
 
 void launch_tet_count(const Launch& L, const Dev& D, int* cnt) {
-    k_tet_count<<<star_blocks(D.n), 32 * WARPS_PER_BLOCK, 0, L.stream>>>(D, cnt);
-    ++*L.launches;
+    // filter-only pass, then the exact pass over the stars it left (count read
+    // on the device), then the queue is emptied
+    cudaMemsetAsync(&D.ctr->exact_next, 0, sizeof(int), L.stream);
+    k_tet_count<false><<<star_blocks(D.n), 32 * WARPS_PER_BLOCK, 0, L.stream>>>(D, cnt);
+    k_tet_count<true><<<star_blocks(D.n, WARPS_PER_BLOCK, 2), 32 * WARPS_PER_BLOCK, 0, L.stream>>>(D, cnt);
+    cudaMemsetAsync(&D.ctr->exact_next, 0, sizeof(int), L.stream);
+    *L.launches += 2;
 }
 
 void launch_tet_write(const Launch& L, const Dev& D, const int* base, g4d_tet* tets, const int* sorted_to_input,
