@@ -522,7 +522,7 @@ g4d_status run_ring(g4d_ctx* ctx, const Dev& D, bool labels) {
     const double range = dkey_inv_host(mm[1]) - dkey_inv_host(mm[0]);
     Ring R;
     R.grid = ctx->b[B_GA].as<uint32_t>();
-    R.cols = Cols<uint32_t>{D.ckey, D.cid, D.colStart, D.colEnd, G};
+    R.cols = Cols<uint32_t>{D.ckey, D.cid, D.colStart, D.colEnd, G, nullptr};
     R.scale = (mm[1] && range > 0) ? (double)(G - 3) / range : 1.0;
     R.cap = (int)cap;
     R.rows = &aux->rows;
@@ -577,7 +577,9 @@ g4d_status run_compute(g4d_ctx* ctx, bool map_to_input) {
     // worksets (repeated with a longer overflow list if theirs ran out)
     for (int attempt = 0;; ++attempt) {
         CK(cudaMemsetAsync(ctx->b[B_BCOUNT].p, 0, sizeof(int) * n, ctx->stream));
-        launch_pairs(L, D, gA);
+        // grid B is free after the x pass: it becomes the voxel -> leader map
+        launch_site_map(L, D, reinterpret_cast<int*>(gB));
+        launch_pairs(L, D, gA, reinterpret_cast<int*>(gB));
         launch_missing(L, D);
         st = run_proposal(ctx, D);
         if (st) return st;
@@ -681,7 +683,7 @@ g4d_status run_wave(g4d_ctx* ctx, const double* d_xyz, const int64_t* offs, cons
     std::vector<int> slot_cloud(cl, cl + ns);
     std::vector<int> list_pos(ns);
     std::stable_sort(slot_cloud.begin(), slot_cloud.end(), [&](int a, int b) { return Gc[a] < Gc[b]; });
-    std::vector<long long> slotIn(ns), slotCol(ns);
+    std::vector<long long> slotIn(ns), slotCol(ns), slotVox(ns);
     std::vector<int> slotW(ns + 1), slotG(ns);
     struct Stack { int G, k0, K; long long col, vox; };
     std::vector<Stack> stacks;
@@ -695,23 +697,26 @@ g4d_status run_wave(g4d_ctx* ctx, const double* d_xyz, const int64_t* offs, cons
         if (stacks.empty() || stacks.back().G != G) stacks.push_back({G, k, 0, cols, voxels});
         stacks.back().K++;
         slotCol[k] = cols;
+        slotVox[k] = voxels;
         cols += (long long)G * G;
         voxels += (long long)G * G * G;
     }
     const int n = slotW[ns];
     ctx->n = n;
-    // device copies of the slot tables: slotIn, slotCol, dst (int64), slotW, slotG, tc (int32)
+    // device copies of the slot tables: slotIn, slotCol, dst, slotVox (int64), slotW, slotG, tc (int32)
     const size_t i64b = sizeof(long long) * ns, i32b = sizeof(int) * (ns + 1);
-    CK(ctx->b[B_SLOTS].ensure(3 * i64b + 3 * i32b + 64));
+    CK(ctx->b[B_SLOTS].ensure(4 * i64b + 3 * i32b + 64));
     char* sb = ctx->b[B_SLOTS].as<char>();
     long long* d_slotIn = reinterpret_cast<long long*>(sb);
     long long* d_slotCol = reinterpret_cast<long long*>(sb + i64b);
     long long* d_dst = reinterpret_cast<long long*>(sb + 2 * i64b);
-    int* d_slotW = reinterpret_cast<int*>(sb + 3 * i64b);
-    int* d_slotG = reinterpret_cast<int*>(sb + 3 * i64b + i32b);
-    int* d_tc = reinterpret_cast<int*>(sb + 3 * i64b + 2 * i32b);
+    long long* d_slotVox = reinterpret_cast<long long*>(sb + 3 * i64b);
+    int* d_slotW = reinterpret_cast<int*>(sb + 4 * i64b);
+    int* d_slotG = reinterpret_cast<int*>(sb + 4 * i64b + i32b);
+    int* d_tc = reinterpret_cast<int*>(sb + 4 * i64b + 2 * i32b);
     CK(cudaMemcpyAsync(d_slotIn, slotIn.data(), i64b, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(d_slotCol, slotCol.data(), i64b, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(d_slotVox, slotVox.data(), i64b, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(d_slotW, slotW.data(), i32b, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(d_slotG, slotG.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, ctx->stream));
 
@@ -788,8 +793,12 @@ g4d_status run_wave(g4d_ctx* ctx, const double* d_xyz, const int64_t* offs, cons
     cudaEventRecord(ctx->ev[2], ctx->stream);
     for (int attempt = 0;; ++attempt) {
         CK(cudaMemsetAsync(ctx->b[B_BCOUNT].p, 0, sizeof(int) * n, ctx->stream));
+        // the grids B are free after the x passes: they become the voxel -> leader maps
+        int* map = reinterpret_cast<int*>(gB);
+        launch_b_site_map(L, ctx->b[B_VOX].as<uint32_t>(), skey, d_slotG, d_slotVox, n, map);
         for (const Stack& S : stacks)
-            launch_pairs_stack(L, D, gA + S.vox, S.G, S.K, ckey, ctx->b[B_CID].as<int>(), cs + S.col, ce + S.col);
+            launch_pairs_stack(L, D, gA + S.vox, map + S.vox, S.G, S.K, ckey, ctx->b[B_CID].as<int>(), cs + S.col,
+                               ce + S.col);
         launch_missing_u64(L, D, skey);
         bool again = false;
         st = worksets_fit(ctx, D, attempt, &again);

@@ -178,11 +178,14 @@ struct Cols {
     const int* start;  // first key of each column of this grid
     const int* end;
     int G;
+    const int* map;    // leader id at every occupied voxel of this grid, or null
 };
 
-// site (packed voxel) -> point id of the voxel's leader (smallest Morton index)
+// site (packed voxel) -> point id of the voxel's leader (smallest Morton index):
+// one load from the voxel map when there is one, else a walk of its column
 template <class KeyT>
 __device__ __forceinline__ int site_to_id(const Cols<KeyT>& C, uint32_t e) {
+    if (C.map) return C.map[((size_t)vz(e) * C.G + vy(e)) * C.G + vx(e)];
     const int c = (int)(vy(e) * (uint32_t)C.G + vx(e));
     const uint32_t z = vz(e);
     for (int j = C.start[c], je = C.end[c]; j < je; ++j)
@@ -238,14 +241,17 @@ void launch_b_localize(const Launch& L, const g4d_tet* in, int ntet, const unsig
 void launch_pba_z(const Launch& L, const Dev& D, uint32_t* out);
 void launch_pba_y(const Launch& L, int G, uint32_t* in, uint32_t* out);
 void launch_pba_x(const Launch& L, int G, uint32_t* in, uint32_t* out);
-void launch_pairs(const Launch& L, const Dev& D, const uint32_t* grid);
+void launch_pairs(const Launch& L, const Dev& D, const uint32_t* grid, int* map);
+void launch_site_map(const Launch& L, const Dev& D, int* map);
+void launch_b_site_map(const Launch& L, const uint32_t* vox, const unsigned long long* skey, const int* slotG,
+                       const long long* slotVox, int n, int* map);
 void launch_missing(const Launch& L, const Dev& D);
 // stacks of K grids of width G (batches; 64-bit column keys)
 void launch_pba_z_stack(const Launch& L, int G, int K, const unsigned long long* ckey, const int* cs, const int* ce,
                         uint32_t* out);
 void launch_pba_y_stack(const Launch& L, int G, int K, uint32_t* in, uint32_t* out);
 void launch_pba_x_stack(const Launch& L, int G, int K, uint32_t* in, uint32_t* out);
-void launch_pairs_stack(const Launch& L, const Dev& D, const uint32_t* stack, int G, int K,
+void launch_pairs_stack(const Launch& L, const Dev& D, const uint32_t* stack, int* map, int G, int K,
                         const unsigned long long* ckey, const int* cid, const int* cs, const int* ce);
 void launch_missing_u64(const Launch& L, const Dev& D, const unsigned long long* mkey);
 

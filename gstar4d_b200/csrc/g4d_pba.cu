@@ -453,6 +453,7 @@ __global__ void __launch_bounds__(32 * PAIR_WARPS) k_pairs(Dev D, const uint32_t
     const uint32_t* grid = stack + (size_t)kk * plane * G;
     C.start += (size_t)kk * plane;
     C.end += (size_t)kk * plane;
+    if (C.map) C.map += (size_t)kk * plane * G;
     const int lane = threadIdx.x, w = threadIdx.y;
     // every lane of the warp walks the same z range so the warp collectives
     // below stay converged; lanes past the grid edge carry no pairs (they read
@@ -612,19 +613,59 @@ void launch_pba_x_stack(const Launch& L, int G, int K, uint32_t* in, uint32_t* o
     ++*L.launches;
 }
 
-void launch_pairs(const Launch& L, const Dev& D, const uint32_t* grid) {
-    const int G = D.G;
-    const int nzc = (G - 1 + PAIR_ZC - 1) / PAIR_ZC;
-    dim3 b(32, PAIR_WARPS), g((G - 1 + 31) / 32, (G - 1 + PAIR_WARPS - 1) / PAIR_WARPS, nzc);
-    k_pairs<<<g, b, 0, L.stream>>>(D, grid, Cols<uint32_t>{D.ckey, D.cid, D.colStart, D.colEnd, G}, nzc);
+// leader id at the voxel of every leader (the first point of its voxel in
+// Morton order), for site_to_id; other voxels of the map are never read
+__global__ void k_site_map(const uint32_t* __restrict__ vox, const uint32_t* __restrict__ mkey, int n, int G,
+                           int* __restrict__ map) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (i > 0 && mkey[i - 1] == mkey[i]) continue;
+        const uint32_t e = vox[i];
+        map[((size_t)vz(e) * G + vy(e)) * G + vx(e)] = i;
+    }
+}
+
+// the same for a batch pass: point i of slot k = skey >> 30 maps into its grid
+// at slotVox[k]; leaders are the first of equal sort keys
+__global__ void k_b_site_map(const uint32_t* __restrict__ vox, const unsigned long long* __restrict__ skey,
+                             const int* __restrict__ slotG, const long long* __restrict__ slotVox, int n,
+                             int* __restrict__ map) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (i > 0 && skey[i - 1] == skey[i]) continue;
+        const int k = (int)(skey[i] >> 30);
+        const size_t G = (size_t)slotG[k];
+        const uint32_t e = vox[i];
+        map[(size_t)slotVox[k] + ((size_t)vz(e) * G + vy(e)) * G + vx(e)] = i;
+    }
+}
+
+void launch_site_map(const Launch& L, const Dev& D, int* map) {
+    int blocks = (D.n + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    k_site_map<<<blocks, 256, 0, L.stream>>>(D.vox, D.mkey, D.n, D.G, map);
     ++*L.launches;
 }
 
-void launch_pairs_stack(const Launch& L, const Dev& D, const uint32_t* stack, int G, int K,
+void launch_b_site_map(const Launch& L, const uint32_t* vox, const unsigned long long* skey, const int* slotG,
+                       const long long* slotVox, int n, int* map) {
+    int blocks = (n + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    k_b_site_map<<<blocks, 256, 0, L.stream>>>(vox, skey, slotG, slotVox, n, map);
+    ++*L.launches;
+}
+
+void launch_pairs(const Launch& L, const Dev& D, const uint32_t* grid, int* map) {
+    const int G = D.G;
+    const int nzc = (G - 1 + PAIR_ZC - 1) / PAIR_ZC;
+    dim3 b(32, PAIR_WARPS), g((G - 1 + 31) / 32, (G - 1 + PAIR_WARPS - 1) / PAIR_WARPS, nzc);
+    k_pairs<<<g, b, 0, L.stream>>>(D, grid, Cols<uint32_t>{D.ckey, D.cid, D.colStart, D.colEnd, G, map}, nzc);
+    ++*L.launches;
+}
+
+void launch_pairs_stack(const Launch& L, const Dev& D, const uint32_t* stack, int* map, int G, int K,
                         const unsigned long long* ckey, const int* cid, const int* cs, const int* ce) {
     const int nzc = (G - 1 + PAIR_ZC - 1) / PAIR_ZC;
     dim3 b(32, PAIR_WARPS), g((G - 1 + 31) / 32, (G - 1 + PAIR_WARPS - 1) / PAIR_WARPS, nzc * K);
-    k_pairs<<<g, b, 0, L.stream>>>(D, stack, Cols<unsigned long long>{ckey, cid, cs, ce, G}, nzc);
+    k_pairs<<<g, b, 0, L.stream>>>(D, stack, Cols<unsigned long long>{ckey, cid, cs, ce, G, map}, nzc);
     ++*L.launches;
 }
 
