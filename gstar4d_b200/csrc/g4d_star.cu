@@ -368,15 +368,12 @@ __device__ __forceinline__ void push_inbox(const Dev& D, int t, int v, bool* ove
 // warp helpers
 // --------------------------------------------------------------------------
 
+// exclusive prefix sum over the warp of v in 0..3 (two ballots of its bits)
 __device__ __forceinline__ int warp_excl_scan(int v, int lane, int* total) {
-    int incl = v;
-#pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
-        const int u = __shfl_up_sync(0xffffffffu, incl, off);
-        if (lane >= off) incl += u;
-    }
-    *total = __shfl_sync(0xffffffffu, incl, 31);
-    return incl - v;
+    const unsigned b0 = __ballot_sync(0xffffffffu, v & 1), b1 = __ballot_sync(0xffffffffu, v & 2);
+    const unsigned below = (1u << lane) - 1u;
+    *total = __popc(b0) + 2 * __popc(b1);
+    return __popc(b0 & below) + 2 * __popc(b1 & below);
 }
 
 // Insert id v into the shared history hash; returns slot, sets *fresh when new.
@@ -443,20 +440,25 @@ __device__ int warp_insert(WS<C>& S, int lane, int s, double3 ps, int sp, int ge
         const bool b = (m >> lane) & 1u;
         if (b) S.blist[prefix + __popc(m & ((1u << lane) - 1u))] = (Idx)t;
         prefix += __popc(m);
-        typename C::Rec rec[3];
-        int ne = 0;
+        // edge i (opposite vertex i) is on the hole boundary when the
+        // triangle across it is not beneath
+        int o[3] = {0, 0, 0};
+        bool e[3] = {false, false, false};
         if (b) {
 #pragma unroll
             for (int i = 0; i < 3; ++i) {
-                const int o = S.to[i][t];
-                const bool ob = (S.bmask[o >> 5] >> (o & 31)) & 1u;
-                if (!ob) rec[ne++] = C::rec(S.tv[(i + 1) % 3][t], S.tv[(i + 2) % 3][t], o, S.tj[i][t]);
+                o[i] = S.to[i][t];
+                e[i] = !((S.bmask[o[i] >> 5] >> (o[i] & 31)) & 1u);
             }
         }
         int total;
-        const int start = nedge + warp_excl_scan(ne, lane, &total);
-        for (int k = 0; k < ne; ++k)
-            if (start + k < C::TS) S.erec[start + k] = rec[k];
+        int k = nedge + warp_excl_scan((int)e[0] + (int)e[1] + (int)e[2], lane, &total);
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+            if (e[i]) {
+                if (k < C::TS) S.erec[k] = C::rec(S.tv[(i + 1) % 3][t], S.tv[(i + 2) % 3][t], o[i], S.tj[i][t]);
+                ++k;
+            }
         nedge += total;
     }
     __syncwarp();
