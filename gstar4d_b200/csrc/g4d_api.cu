@@ -54,7 +54,7 @@ enum BufId {
     B_WLEMIT, B_WLEMIT2, B_DROWN, B_DROWN2, B_CTR, B_CNT, B_BASE, B_TETS, B_CUB, B_BAD, B_LIDX, B_LHH, B_LTRI,
     B_WLINSL, B_WLPROM, B_SKEY0, B_SKEY, B_GIDX, B_LOCAL, B_BCKEY0, B_BCKEY, B_SLOTS, B_MMB, B_TC, B_TETS2, B_OVF, B_OVF2, B_KMASK, B_BOUT, B_OCC, B_WLEXACT, B_WLBIG,
     B_MLP_P, B_MLP_G, B_MLP_M1, B_MLP_M2, B_MLP_AUX, B_RING_PAIR, B_RING_X, B_RING_Y, B_RING_LOGIT, B_TILES,
-    B_DIAG_X, B_DIAG_Y, B_DIAG_P, B_DIAG_G, B_FIX, B_NUM
+    B_DIAG_X, B_DIAG_Y, B_DIAG_P, B_DIAG_G, B_FIX, B_FACE, B_NUM
 };
 
 }  // namespace
@@ -472,7 +472,9 @@ g4d_status run_extract(g4d_ctx* ctx, const Dev& D, const int* sorted_to_input) {
     CK(ctx->b[B_TETS].ensure(sizeof(g4d_tet) * (size_t)std::max(ntet, 1)));
     // at most one queued link per (tetrahedron, vertex slot)
     CK(ctx->b[B_FIX].ensure(sizeof(int2) * 4 * (size_t)std::max(ntet, 1)));
-    launch_tet_write(L, D, base, ctx->b[B_TETS].as<g4d_tet>(), sorted_to_input, ctx->b[B_FIX].as<int2>());
+    CK(ctx->b[B_FACE].ensure(sizeof(int4) * (size_t)std::max(ntet, 1)));
+    launch_tet_write(L, D, base, ctx->b[B_TETS].as<g4d_tet>(), sorted_to_input, ctx->b[B_FACE].as<int4>(), ntet,
+                     ctx->b[B_FIX].as<int2>());
     launch_tet_fix(L, D, ctx->b[B_TETS].as<g4d_tet>(), ctx->b[B_FIX].as<int2>());
     cudaEventRecord(ctx->ev[5], ctx->stream);
     Counters h{};

@@ -271,7 +271,7 @@ void launch_proof(const Launch& L, const Dev& D, int count);
 void launch_check(const Launch& L, const Dev& D, unsigned long long* bad);
 void launch_tet_count(const Launch& L, const Dev& D, int* cnt);
 void launch_tet_write(const Launch& L, const Dev& D, const int* base, g4d_tet* tets, const int* sorted_to_input,
-                      int2* fix);
+                      int4* face, int ntet, int2* fix);
 void launch_tet_fix(const Launch& L, const Dev& D, g4d_tet* tets, const int2* fix);
 // learned star proposal (g4d_mlp.cu, g4d_proposal.cu)
 constexpr int MLP_NPARAMS = 9473;

@@ -1418,7 +1418,7 @@ __device__ int face_neighbor(const Dev& D, const int* base, int2* fix, int self,
 // tetrahedra owned by star s (a warp)
 template <class C>
 __device__ __forceinline__ void write_star(const Dev& D, const int* base, g4d_tet* tets, const int* sorted_to_input,
-                                           int2* fix, int s, int ntri, const int* ids, const typename C::Tri* gt,
+                                           int4* face, int s, int ntri, const int* ids, const typename C::Tri* gt,
                                            uint16_t* rank, int lane) {
     int pre = 0;
     for (int b0 = 0; b0 < ntri; b0 += 32) {
@@ -1447,7 +1447,8 @@ __device__ __forceinline__ void write_star(const Dev& D, const int* base, g4d_te
             // a neighbour owned by x < s is linked by x's side
             out.opp[i] = (x > s && C::kept(N)) ? base[s] + rank[oi] : -1;
         }
-        out.opp[3] = face_neighbor(D, base, fix, base[s] + rank[t], s, v[0], v[1], v[2]);
+        out.opp[3] = -1;  // k_tet_face3
+        face[base[s] + rank[t]] = make_int4(s, v[0], v[1], v[2]);
         if (sorted_to_input) {
             out.v[0] = sorted_to_input[v[0]];
             out.v[1] = sorted_to_input[v[1]];
@@ -1466,7 +1467,7 @@ __device__ __forceinline__ void write_star(const Dev& D, const int* base, g4d_te
 // about one remote lookup of latency instead of four), then each lane writes
 // whole tetrahedra. buf: 128 B ranks, 128 B kept list, 4 ints per kept triangle.
 __device__ __forceinline__ void write_star_small(const Dev& D, const int* base, g4d_tet* tets,
-                                                 const int* sorted_to_input, int2* fix, int s, int ntri,
+                                                 const int* sorted_to_input, int4* face, int s, int ntri,
                                                  const int* ids, const uint2* gt, uint8_t* buf, int lane) {
     uint8_t* rank = buf;
     uint8_t* kt = buf + 128;
@@ -1483,26 +1484,20 @@ __device__ __forceinline__ void write_star_small(const Dev& D, const int* base, 
     }
     __syncwarp();
     const int bs = base[s];
-    for (int k = lane; k < 4 * nk; k += 32) {
-        const int f = k & 3;
-        const uint2 T = gt[kt[k >> 2]];
+    for (int k = lane; k < 3 * nk; k += 32) {
+        const int r3 = k / 3, f = k - 3 * r3;
+        const uint2 T = gt[kt[r3]];
         const int s0 = SmallStar::tv(T, 0), s1 = SmallStar::tv(T, 1), s2 = SmallStar::tv(T, 2);
         const int v0 = ids[s0] & (int)HID, v1 = ids[s1] & (int)HID, v2 = ids[s2] & (int)HID;
-        int o;
-        if (f < 3) {
-            // across the face (s, v[f+1], v[f+2]): the adjacent link triangle
-            const int oi = SmallStar::to(T, f);
-            const uint2 N = gt[oi];
-            const int e1 = f == 0 ? s1 : (f == 1 ? s2 : s0), e2 = f == 0 ? s2 : (f == 1 ? s0 : s1);
-            const int n0 = SmallStar::tv(N, 0), n1 = SmallStar::tv(N, 1), n2 = SmallStar::tv(N, 2);
-            const int xs = (n2 != e1 && n2 != e2) ? n2 : ((n1 != e1 && n1 != e2) ? n1 : n0);
-            const int x = ids[xs] & (int)HID;
-            // a neighbour owned by x < s is linked by x's side
-            o = (x > s && SmallStar::kept(N)) ? bs + rank[oi] : -1;
-        } else {
-            o = face_neighbor(D, base, fix, bs + (k >> 2), s, v0, v1, v2);
-        }
-        opp[k] = o;
+        // across the face (s, v[f+1], v[f+2]): the adjacent link triangle
+        const int oi = SmallStar::to(T, f);
+        const uint2 N = gt[oi];
+        const int e1 = f == 0 ? s1 : (f == 1 ? s2 : s0), e2 = f == 0 ? s2 : (f == 1 ? s0 : s1);
+        const int n0 = SmallStar::tv(N, 0), n1 = SmallStar::tv(N, 1), n2 = SmallStar::tv(N, 2);
+        const int xs = (n2 != e1 && n2 != e2) ? n2 : ((n1 != e1 && n1 != e2) ? n1 : n0);
+        const int x = ids[xs] & (int)HID;
+        // a neighbour owned by x < s is linked by x's side
+        opp[k] = (x > s && SmallStar::kept(N)) ? bs + rank[oi] : -1;
     }
     __syncwarp();
     for (int r = lane; r < nk; r += 32) {
@@ -1518,16 +1513,17 @@ __device__ __forceinline__ void write_star_small(const Dev& D, const int* base, 
         } else {
             out.v[0] = v0; out.v[1] = v1; out.v[2] = v2; out.v[3] = s;
         }
-        out.opp[0] = opp[4 * r];
-        out.opp[1] = opp[4 * r + 1];
-        out.opp[2] = opp[4 * r + 2];
-        out.opp[3] = opp[4 * r + 3];
+        out.opp[0] = opp[3 * r];
+        out.opp[1] = opp[3 * r + 1];
+        out.opp[2] = opp[3 * r + 2];
+        out.opp[3] = -1;  // k_tet_face3
         tets[bs + r] = out;
+        face[bs + r] = make_int4(s, v0, v1, v2);
     }
 }
 
 __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_tet_write(Dev D, const int* base, g4d_tet* tets,
-                                                                    const int* sorted_to_input, int2* fix) {
+                                                                    const int* sorted_to_input, int4* face) {
     __shared__ int shh[WARPS_PER_BLOCK][HSLOTS];
     // large stars: triangle ranks; small stars: write_star_small's buffer
     __shared__ __align__(16) uint16_t srank[WARPS_PER_BLOCK][LTSTRIDE];
@@ -1541,11 +1537,23 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_tet_write(Dev D, const
         const StarView V = star_view(D, s);
         const int* ids = stage_ids(V, shh[threadIdx.x >> 5], lane);
         if (!V.large)
-            write_star_small(D, base, tets, sorted_to_input, fix, s, h.ntri, ids, static_cast<const uint2*>(V.tri),
+            write_star_small(D, base, tets, sorted_to_input, face, s, h.ntri, ids, static_cast<const uint2*>(V.tri),
                              reinterpret_cast<uint8_t*>(rank), lane);
         else
-            write_star<LargeStar>(D, base, tets, sorted_to_input, fix, s, h.ntri, ids,
+            write_star<LargeStar>(D, base, tets, sorted_to_input, face, s, h.ntri, ids,
                                   static_cast<const uint4*>(V.tri), rank, lane);
+    }
+}
+
+// the link across the face opposite the owner, one tetrahedron per thread
+// (item: owner s and the other three vertices, written by k_tet_write); every
+// lane does a remote lookup, so they overlap
+__global__ void k_tet_face3(Dev D, const int* __restrict__ base, g4d_tet* tets, const int4* __restrict__ face,
+                            int ntet, int2* fix) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntet; t += gridDim.x * blockDim.x) {
+        const int4 it = face[t];
+        const int o = face_neighbor(D, base, fix, t, it.x, it.y, it.z, it.w);
+        if (o >= 0) tets[t].opp[3] = o;
     }
 }
 
@@ -1703,10 +1711,14 @@ void launch_tet_count(const Launch& L, const Dev& D, int* cnt) {
 }
 
 void launch_tet_write(const Launch& L, const Dev& D, const int* base, g4d_tet* tets, const int* sorted_to_input,
-                      int2* fix) {
+                      int4* face, int ntet, int2* fix) {
     cudaMemsetAsync(&D.ctr->fix_next, 0, sizeof(int), L.stream);
-    k_tet_write<<<star_blocks(D.n), 32 * WARPS_PER_BLOCK, 0, L.stream>>>(D, base, tets, sorted_to_input, fix);
-    ++*L.launches;
+    k_tet_write<<<star_blocks(D.n), 32 * WARPS_PER_BLOCK, 0, L.stream>>>(D, base, tets, sorted_to_input, face);
+    int blocks = (ntet + 255) / 256;
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    if (blocks < 1) blocks = 1;
+    k_tet_face3<<<blocks, 256, 0, L.stream>>>(D, base, tets, face, ntet, fix);
+    *L.launches += 2;
 }
 
 void launch_tet_fix(const Launch& L, const Dev& D, g4d_tet* tets, const int2* fix) {
