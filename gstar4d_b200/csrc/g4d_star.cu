@@ -128,7 +128,7 @@ struct WS {
     int nedge, nfree, ntri, nins, nhist, ncoord;
 };
 
-// 4 blocks of 4 warps per SM: 16 images plus the per-block reservation in 228 KB
+// MINB_FAST blocks of 4 warps per SM: their images plus the per-block reservation in 228 KB
 static_assert(SmallStar::MINB_FAST * (4 * sizeof(WS<SmallStar>) + 1024) <= 228 * 1024, "small star image too large");
 static_assert(sizeof(WS<LargeStar>) + 1024 <= 227 * 1024, "large star image too large");
 
