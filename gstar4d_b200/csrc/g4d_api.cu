@@ -64,6 +64,8 @@ struct g4d_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaStream_t copy_stream = nullptr;  // batch results to host while the next pass computes
+    cudaStream_t side = nullptr;         // proofs beside emission
+    cudaEvent_t fork = nullptr, join = nullptr;
     Buf b[B_NUM];
     std::string err;
     // results of the last compute
@@ -386,9 +388,18 @@ g4d_status run_splay(g4d_ctx* ctx, Dev& D) {
         // emission phase; it only adds (deduplicated) inbox requests, so when the
         // overflow list ran out it is grown and the phase repeated
         for (int attempt = 0;; ++attempt) {
+            // proofs on the side stream next to emission: both only add
+            // deduplicated inbox requests
+            if (drownCount) {
+                CK(cudaEventRecord(ctx->fork, ctx->stream));
+                CK(cudaStreamWaitEvent(ctx->side, ctx->fork, 0));
+                Launch Ls{ctx->side, &ctx->launches};
+                launch_proof(Ls, D, drownCount);
+                CK(cudaEventRecord(ctx->join, ctx->side));
+            }
             if (ovfCount) launch_requeue(L, D, ovfCount);
-            if (drownCount) launch_proof(L, D, drownCount);
             if (emitCount) launch_emit(L, D, emitCount);
+            if (drownCount) CK(cudaStreamWaitEvent(ctx->stream, ctx->join, 0));
             CK(cudaMemcpyAsync(&h, dctr, sizeof(Counters), cudaMemcpyDeviceToHost, ctx->stream));
             CK(cudaStreamSynchronize(ctx->stream));
             if (!(h.err & ERR_OVFCAP) || attempt >= 3) break;
@@ -1106,7 +1117,13 @@ g4d_status g4d_create(g4d_ctx** out, const g4d_config* cfg) {
         delete ctx;
         return G4D_ERR_CUDA;
     }
-    if (cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    if (cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->join, cudaEventDisableTiming) != cudaSuccess) {
+        if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
+        if (ctx->side) cudaStreamDestroy(ctx->side);
+        if (ctx->fork) cudaEventDestroy(ctx->fork);
         cudaStreamDestroy(ctx->stream);
         delete ctx;
         return G4D_ERR_CUDA;
@@ -1121,9 +1138,13 @@ void g4d_destroy(g4d_ctx* ctx) {
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
+    if (ctx->side) cudaStreamSynchronize(ctx->side);
     for (auto& b : ctx->b) b.release();
     for (auto& e : ctx->ev) cudaEventDestroy(e);
+    if (ctx->fork) cudaEventDestroy(ctx->fork);
+    if (ctx->join) cudaEventDestroy(ctx->join);
     if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
+    if (ctx->side) cudaStreamDestroy(ctx->side);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
