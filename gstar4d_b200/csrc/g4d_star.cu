@@ -788,7 +788,27 @@ __global__ void __launch_bounds__(32 * C::WARPS, EXACT ? C::MINB : C::MINB_FAST)
             atomicOr(&S.insMask[slot >> 5], 1u << (slot & 31));
         }
         __syncwarp();
-        warp_sort_order(S, lane, nins);
+        if (nins <= 32) {
+            // one candidate per lane: bitonic sort in registers by (distance,
+            // slot), padded with +inf
+            float key = lane < nins ? S.okey[lane] : 3.0e38f;
+            int slot = lane < nins ? (int)S.order[lane] : 0x7fffffff;
+#pragma unroll
+            for (int k = 2; k <= 32; k <<= 1)
+#pragma unroll
+                for (int j = k >> 1; j > 0; j >>= 1) {
+                    const float ok = __shfl_xor_sync(0xffffffffu, key, j);
+                    const int os = __shfl_xor_sync(0xffffffffu, slot, j);
+                    const bool other_less = ok < key || (ok == key && os < slot);
+                    // the lower lane of a pair keeps the smaller in an ascending block
+                    const bool keep_small = ((lane & j) == 0) == ((lane & k) == 0);
+                    if (keep_small == other_less) { key = ok; slot = os; }
+                }
+            __syncwarp();
+            if (lane < nins) S.order[lane] = (typename C::Slot)slot;
+        } else {
+            warp_sort_order(S, lane, nins);
+        }
         if (lane == 0) S.nhist = nins;
         __syncwarp();
         const int gen = 1;
