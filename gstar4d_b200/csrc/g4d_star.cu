@@ -403,63 +403,105 @@ __device__ int warp_insert(WS<C>& S, int lane, int s, double3 ps, int sp, int ge
     const double3 pp = wpt(S, sp);
     const int pid = wid(S, sp);
     const int ntri = S.ntri;
-    int nb = 0, nalive = 0;
-    bool undecided = false;
-    for (int base = 0; base < ntri; base += 32) {
-        const int t = base + lane;
+    int nb = 0, nedge = 0;
+    if (ntri <= 32) {
+        // one chunk (the common case): the beneath mask, the triangle's
+        // vertices and neighbours stay in registers for the boundary pass
+        const int t = lane;
         bool b = false, al = false, und = false;
+        int a = 0, bb = 0, c = 0;
         if (t < ntri && (S.tf[t] & 0x80)) {
             al = true;
-            const int a = S.tv[0][t], bb = S.tv[1][t], c = S.tv[2][t];
+            a = S.tv[0][t]; bb = S.tv[1][t]; c = S.tv[2][t];
             const int sg = pred4<EXACT>(wpt(S, a), wpt(S, bb), wpt(S, c), ps, pp, wid(S, a), wid(S, bb), wid(S, c),
                                         s, pid, sink, exact);
             b = sg < 0;
             und = sg == 0;
         }
         const unsigned m = __ballot_sync(0xffffffffu, b);
-        nalive += __popc(__ballot_sync(0xffffffffu, al));
-        if (!EXACT) undecided |= __any_sync(0xffffffffu, und);
-        if (lane == 0) S.bmask[base >> 5] = m;
-        nb += __popc(m);
-    }
-    __syncwarp();
-    if (!EXACT && undecided) return -3;
-    if (nb == 0) return 0;
-    if (nb == nalive) {
-        if (lane == 0) {
-            atomicOr(err, ERR_TOPOLOGY);
-            G4D_TRACE("star %d: point %d beneath all %d triangles\n", s, pid, nalive);
+        const int nalive = __popc(__ballot_sync(0xffffffffu, al));
+        if (!EXACT && __any_sync(0xffffffffu, und)) return -3;
+        nb = __popc(m);
+        if (nb == 0) return 0;
+        if (nb == nalive) {
+            if (lane == 0) {
+                atomicOr(err, ERR_TOPOLOGY);
+                G4D_TRACE("star %d: point %d beneath all %d triangles\n", s, pid, nalive);
+            }
+            return -1;
         }
-        return -1;
-    }
-    // beneath triangles in index order, and the hole's boundary edges
-    int nedge = 0, prefix = 0;
-    for (int base = 0; base < ntri; base += 32) {
-        const unsigned m = S.bmask[base >> 5];
-        const int t = base + lane;
-        const bool b = (m >> lane) & 1u;
-        if (b) S.blist[prefix + __popc(m & ((1u << lane) - 1u))] = (Idx)t;
-        prefix += __popc(m);
-        // edge i (opposite vertex i) is on the hole boundary when the
-        // triangle across it is not beneath
-        int o[3] = {0, 0, 0};
-        bool e[3] = {false, false, false};
+        if (lane == 0) S.bmask[0] = m;
+        int o0 = 0, o1 = 0, o2 = 0;
+        bool e0 = false, e1 = false, e2 = false;
         if (b) {
-#pragma unroll
-            for (int i = 0; i < 3; ++i) {
-                o[i] = S.to[i][t];
-                e[i] = !((S.bmask[o[i] >> 5] >> (o[i] & 31)) & 1u);
-            }
+            S.blist[__popc(m & ((1u << lane) - 1u))] = (Idx)t;
+            o0 = S.to[0][t]; o1 = S.to[1][t]; o2 = S.to[2][t];
+            e0 = !((m >> o0) & 1u); e1 = !((m >> o1) & 1u); e2 = !((m >> o2) & 1u);
         }
-        int total;
-        int k = nedge + warp_excl_scan((int)e[0] + (int)e[1] + (int)e[2], lane, &total);
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-            if (e[i]) {
-                if (k < C::TS) S.erec[k] = C::rec(S.tv[(i + 1) % 3][t], S.tv[(i + 2) % 3][t], o[i], S.tj[i][t]);
-                ++k;
+        int k = warp_excl_scan((int)e0 + (int)e1 + (int)e2, lane, &nedge);
+        // edge i is the one opposite vertex i
+        if (e0) { if (k < C::TS) S.erec[k] = C::rec(bb, c, o0, S.tj[0][t]); ++k; }
+        if (e1) { if (k < C::TS) S.erec[k] = C::rec(c, a, o1, S.tj[1][t]); ++k; }
+        if (e2) { if (k < C::TS) S.erec[k] = C::rec(a, bb, o2, S.tj[2][t]); }
+    } else {
+        int nalive = 0;
+        bool undecided = false;
+        for (int base = 0; base < ntri; base += 32) {
+            const int t = base + lane;
+            bool b = false, al = false, und = false;
+            if (t < ntri && (S.tf[t] & 0x80)) {
+                al = true;
+                const int a = S.tv[0][t], bb = S.tv[1][t], c = S.tv[2][t];
+                const int sg = pred4<EXACT>(wpt(S, a), wpt(S, bb), wpt(S, c), ps, pp, wid(S, a), wid(S, bb), wid(S, c),
+                                            s, pid, sink, exact);
+                b = sg < 0;
+                und = sg == 0;
             }
-        nedge += total;
+            const unsigned m = __ballot_sync(0xffffffffu, b);
+            nalive += __popc(__ballot_sync(0xffffffffu, al));
+            if (!EXACT) undecided |= __any_sync(0xffffffffu, und);
+            if (lane == 0) S.bmask[base >> 5] = m;
+            nb += __popc(m);
+        }
+        __syncwarp();
+        if (!EXACT && undecided) return -3;
+        if (nb == 0) return 0;
+        if (nb == nalive) {
+            if (lane == 0) {
+                atomicOr(err, ERR_TOPOLOGY);
+                G4D_TRACE("star %d: point %d beneath all %d triangles\n", s, pid, nalive);
+            }
+            return -1;
+        }
+        // beneath triangles in index order, and the hole's boundary edges
+        int prefix = 0;
+        for (int base = 0; base < ntri; base += 32) {
+            const unsigned m = S.bmask[base >> 5];
+            const int t = base + lane;
+            const bool b = (m >> lane) & 1u;
+            if (b) S.blist[prefix + __popc(m & ((1u << lane) - 1u))] = (Idx)t;
+            prefix += __popc(m);
+            // edge i (opposite vertex i) is on the hole boundary when the
+            // triangle across it is not beneath
+            int o[3] = {0, 0, 0};
+            bool e[3] = {false, false, false};
+            if (b) {
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    o[i] = S.to[i][t];
+                    e[i] = !((S.bmask[o[i] >> 5] >> (o[i] & 31)) & 1u);
+                }
+            }
+            int total;
+            int k = nedge + warp_excl_scan((int)e[0] + (int)e[1] + (int)e[2], lane, &total);
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+                if (e[i]) {
+                    if (k < C::TS) S.erec[k] = C::rec(S.tv[(i + 1) % 3][t], S.tv[(i + 2) % 3][t], o[i], S.tj[i][t]);
+                    ++k;
+                }
+            nedge += total;
+        }
     }
     __syncwarp();
     const int B = nedge;
