@@ -535,7 +535,8 @@ g4d_status run_ring(g4d_ctx* ctx, const Dev& D, bool labels) {
     const double range = dkey_inv_host(mm[1]) - dkey_inv_host(mm[0]);
     Ring R;
     R.grid = ctx->b[B_GA].as<uint32_t>();
-    R.cols = Cols<uint32_t>{D.ckey, D.cid, D.colStart, D.colEnd, G, nullptr};
+    // grid B holds the voxel -> leader map from the pair scan of this cloud
+    R.cols = Cols<uint32_t>{D.ckey, D.cid, D.colStart, D.colEnd, G, ctx->b[B_GB].as<int>()};
     R.scale = (mm[1] && range > 0) ? (double)(G - 3) / range : 1.0;
     R.cap = (int)cap;
     R.rows = &aux->rows;
