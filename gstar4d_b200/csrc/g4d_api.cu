@@ -413,6 +413,11 @@ g4d_status run_splay(g4d_ctx* ctx, Dev& D) {
         st = check_err(ctx, h.err);
         if (st) return st;
         if (h.ins_count == 0 && h.ins_count_large == 0) break;
+        if (loops == 0 && D.anyLarge && h.ins_count) {
+            // requests queued during the build may target stars built large
+            launch_reroute(L, D, h.ins_count);
+            if ((st = read())) return st;
+        }
         ovfCount = h.ovf_next;  // requests that found a full inbox this round
         if (h.ins_count) launch_star_insert(L, D, D.wlIns, h.ins_count, false);
         if (h.ins_count_large) launch_star_insert_large(L, D, D.wlInsL, std::min(h.ins_count_large, D.largeCap));

@@ -268,6 +268,7 @@ void launch_promote(const Launch& L, const Dev& D, int count);
 void launch_requeue(const Launch& L, const Dev& D, int count);
 void launch_emit(const Launch& L, const Dev& D, int count);
 void launch_proof(const Launch& L, const Dev& D, int count);
+void launch_reroute(const Launch& L, const Dev& D, int count);
 void launch_check(const Launch& L, const Dev& D, unsigned long long* bad);
 void launch_tet_count(const Launch& L, const Dev& D, int* cnt);
 void launch_tet_write(const Launch& L, const Dev& D, const int* base, g4d_tet* tets, const int* sorted_to_input,

@@ -902,6 +902,7 @@ __global__ void __launch_bounds__(32 * C::WARPS, EXACT ? C::MINB : C::MINB_FAST)
     for (int w = blockIdx.x * C::WARPS + (threadIdx.x >> 5); w < count; w += warps) {
         __syncwarp();  // the previous item's shared-memory reads are done
         const int s = list[w];
+        if (s < 0) continue;  // moved to the large class's list (k_reroute)
         const StarHdr h = D.hdr[s];
         warp_load(S, D, lane, s, h);
         const double3 ps = gpt(D, s);
@@ -1086,6 +1087,20 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_emit(Dev D, int count)
                 }
         }
         if (__ballot_sync(0xffffffffu, ovf) && lane == 0) atomicOr(&D.ctr->overflow, 1);
+    }
+}
+
+// Requests queued while the initial stars were built (pumping) were routed
+// before some of their stars were built in the large class: such entries move
+// from the small-class list to the large-class list.
+__global__ void k_reroute(Dev D, int count) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const int s = D.wlIns[i];
+        if (s < 0 || D.lidx[s] < 0) continue;
+        D.wlIns[i] = -1;
+        const int q = atomicAdd(&D.ctr->ins_count_large, 1);
+        if (q < D.largeCap) D.wlInsL[q] = s;
+        else atomicOr(&D.ctr->err, ERR_CAPACITY);
     }
 }
 
@@ -1744,6 +1759,13 @@ void launch_requeue(const Launch& L, const Dev& D, int count) {
 
 void launch_emit(const Launch& L, const Dev& D, int count) {
     k_emit<<<star_blocks(count), 32 * WARPS_PER_BLOCK, 0, L.stream>>>(D, count);
+    ++*L.launches;
+}
+
+void launch_reroute(const Launch& L, const Dev& D, int count) {
+    int blocks = (count + 255) / 256;
+    if (blocks > 148 * 4) blocks = 148 * 4;
+    k_reroute<<<blocks, 256, 0, L.stream>>>(D, count);
     ++*L.launches;
 }
 
