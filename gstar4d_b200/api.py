@@ -59,7 +59,8 @@ TET_DTYPE = np.dtype([("v", np.int32, 4), ("opp", np.int32, 4)])
 _lib = None
 
 EXPORTS = ["g4d_default_config", "g4d_create", "g4d_destroy", "g4d_last_error", "g4d_status_string",
-           "g4d_triangulate", "g4d_triangulate_to", "g4d_triangulate_device", "g4d_gdel_init",
+           "g4d_triangulate", "g4d_triangulate_to", "g4d_triangulate_to_f32", "g4d_triangulate_device",
+           "g4d_gdel_init",
            "g4d_gdel_compute", "g4d_get_tetra", "g4d_gdel_deinit", "g4d_get_stats", "g4d_triangulate_batch",
            "g4d_triangulate_batch_to", "g4d_triangulate_batch_device", "g4d_stream",
            "g4d_eval_predicates", "g4d_voronoi", "g4d_voronoi_noalloc", "g4d_proposal_train",
@@ -85,6 +86,7 @@ def load():
     L.g4d_last_error.restype = ctypes.c_char_p
     L.g4d_status_string.restype = ctypes.c_char_p
     L.g4d_triangulate_to.argtypes = [vp, vp, ip, vp, ip, ctypes.POINTER(ip), vp, ctypes.POINTER(Stats)]
+    L.g4d_triangulate_to_f32.argtypes = [vp, vp, ip, vp, ip, ctypes.POINTER(ip), vp, ctypes.POINTER(Stats)]
     L.g4d_triangulate.argtypes = [vp, vp, ip, ctypes.POINTER(vp), ctypes.POINTER(ip), vp, ctypes.POINTER(Stats)]
     L.g4d_triangulate_device.argtypes = [vp, vp, ip, ctypes.POINTER(vp), ctypes.POINTER(ip), ctypes.POINTER(Stats)]
     L.g4d_gdel_init.argtypes = [vp, vp, vp, ip]
@@ -167,12 +169,28 @@ class Triangulator:
     def triangulate(self, points, out=None, want_order=False):
         """points: (n,3) float64 in input order. Returns (tets, order, stats):
         tets structured array (v[4], opp[4]) — or `out` filled in place —, the
-        Morton order (sorted position -> input index) when want_order."""
-        pts = np.ascontiguousarray(points, dtype=np.float64)
-        n = len(pts)
+        Morton order (sorted position -> input index) when want_order. float32
+        points go through g4d_triangulate_to_f32 (widened on the device)."""
+        n = len(points)
         nt = ctypes.c_int(0)
         order = np.empty(n, np.int32) if want_order else None
         stats = Stats()
+        if getattr(points, "dtype", None) == np.float32:
+            pts32 = np.ascontiguousarray(points, dtype=np.float32)
+            own = out is None
+            if own:  # about 6.8 tetrahedra per point; retried at the exact size if exceeded
+                out = np.empty(int(7.5 * n) + 64, TET_DTYPE)
+            st = self._lib.g4d_triangulate_to_f32(self._h, _ptr(pts32), n, _ptr(out), len(out), ctypes.byref(nt),
+                                                  _ptr(order) if want_order else None, ctypes.byref(stats))
+            if own and st == 1 and nt.value > len(out):
+                out = np.empty(nt.value, TET_DTYPE)
+                st = self._lib.g4d_triangulate_to_f32(self._h, _ptr(pts32), n, _ptr(out), len(out),
+                                                      ctypes.byref(nt), _ptr(order) if want_order else None,
+                                                      ctypes.byref(stats))
+            self._check(st)
+            self.last_stats = stats.as_dict()
+            return out[:nt.value], order, self.last_stats
+        pts = np.ascontiguousarray(points, dtype=np.float64)
         if out is None:
             tp = ctypes.c_void_p()
             st = self._lib.g4d_triangulate(self._h, _ptr(pts), n, ctypes.byref(tp), ctypes.byref(nt),

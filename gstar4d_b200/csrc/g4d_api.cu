@@ -54,7 +54,7 @@ enum BufId {
     B_WLEMIT, B_WLEMIT2, B_DROWN, B_DROWN2, B_CTR, B_CNT, B_BASE, B_TETS, B_CUB, B_BAD, B_LIDX, B_LHH, B_LTRI,
     B_WLINSL, B_WLPROM, B_SKEY0, B_SKEY, B_GIDX, B_LOCAL, B_BCKEY0, B_BCKEY, B_SLOTS, B_MMB, B_TC, B_TETS2, B_OVF, B_OVF2, B_KMASK, B_BOUT, B_OCC, B_WLEXACT, B_WLBIG,
     B_MLP_P, B_MLP_G, B_MLP_M1, B_MLP_M2, B_MLP_AUX, B_RING_PAIR, B_RING_X, B_RING_Y, B_RING_LOGIT, B_TILES,
-    B_DIAG_X, B_DIAG_Y, B_DIAG_P, B_DIAG_G, B_FIX, B_FACE, B_NUM
+    B_DIAG_X, B_DIAG_Y, B_DIAG_P, B_DIAG_G, B_FIX, B_FACE, B_XYZ32, B_NUM
 };
 
 }  // namespace
@@ -1199,6 +1199,42 @@ g4d_status g4d_triangulate_to(g4d_ctx* ctx, const double* xyz, int n, g4d_tet* o
     }
     CK(ctx->b[B_XYZ].ensure(sizeof(double) * 3 * (size_t)n));
     CK(cudaMemcpyAsync(ctx->b[B_XYZ].p, xyz, sizeof(double) * 3 * (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
+    st = run_all_device(ctx, ctx->b[B_XYZ].as<double>(), nullptr, n, ctx->cfg.index_space == 0);
+    if (st) return st;
+    *ntet = ctx->ntet;
+    if (out) {
+        if (cap < ctx->ntet) return fail(ctx, G4D_ERR_ARG, "output buffer too small (%d < %d)", cap, ctx->ntet);
+        CK(cudaMemcpyAsync(out, ctx->b[B_TETS].p, sizeof(g4d_tet) * (size_t)ctx->ntet, cudaMemcpyDeviceToHost,
+                           ctx->stream));
+    }
+    if (sorted_to_input)
+        CK(cudaMemcpyAsync(sorted_to_input, ctx->b[B_ORDER].p, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost,
+                           ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (stats) *stats = ctx->stats;
+    return G4D_OK;
+}
+
+g4d_status g4d_triangulate_to_f32(g4d_ctx* ctx, const float* xyz, int n, g4d_tet* out, int cap, int* ntet,
+                                  int* sorted_to_input, g4d_stats* stats) {
+    g4d_status st = check_n(ctx, n);
+    if (st) return st;
+    if (!xyz || !ntet) return fail(ctx, G4D_ERR_ARG, "null argument");
+    cudaSetDevice(ctx->device);
+    Launch L{ctx->stream, &ctx->launches};
+    // float points (the reference's default RealType) are widened on the
+    // device; the triangulation is that of the same values in double
+    CK(ctx->b[B_XYZ32].ensure(sizeof(float) * 3 * (size_t)n));
+    CK(ctx->b[B_XYZ].ensure(sizeof(double) * 3 * (size_t)n));
+    CK(cudaMemcpyAsync(ctx->b[B_XYZ32].p, xyz, sizeof(float) * 3 * (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
+    launch_f32_to_f64(L, ctx->b[B_XYZ32].as<float>(), 3 * (size_t)n, ctx->b[B_XYZ].as<double>());
+    if (ctx->cfg.grid_size < 0) {
+        // autotuned mode: the tuned width for this size and distribution
+        std::vector<double> h(3 * (size_t)n);
+        for (size_t i = 0; i < h.size(); ++i) h[i] = xyz[i];
+        const auto it = ctx->tuned.find(tune_key(n, class_of(occupancy(h.data(), n), n)));
+        if (it != ctx->tuned.end()) ctx->next_grid = it->second;
+    }
     st = run_all_device(ctx, ctx->b[B_XYZ].as<double>(), nullptr, n, ctx->cfg.index_space == 0);
     if (st) return st;
     *ntet = ctx->ntet;

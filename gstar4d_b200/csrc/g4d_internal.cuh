@@ -221,6 +221,7 @@ void launch_gather(const Launch& L, const double* xyz, const uint32_t* vox_in, c
                    double4* P, uint32_t* vox, int* sorted_to_input);
 void launch_colkeys(const Launch& L, const uint32_t* vox, int n, int G, uint32_t* ckey, int* cid);
 void launch_colranges(const Launch& L, const uint32_t* ckey, int n, int G, int* colStart, int* colEnd);
+void launch_f32_to_f64(const Launch& L, const float* in, size_t count, double* out);
 
 // batches (see g4d_order.cu)
 void launch_b_order(const Launch& L, const double* xyz, int nslots, const long long* slotIn, const int* slotW,

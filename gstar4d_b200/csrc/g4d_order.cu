@@ -247,6 +247,19 @@ __global__ void k_b_colkeys(const uint32_t* __restrict__ vox, const unsigned lon
     }
 }
 
+// float coordinates widened to double (exact: every float is a double)
+__global__ void k_f32_to_f64(const float* __restrict__ in, size_t count, double* __restrict__ out) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < count; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = (double)in[i];
+}
+
+void launch_f32_to_f64(const Launch& L, const float* in, size_t count, double* out) {
+    size_t blocks = (count + 255) / 256;
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    k_f32_to_f64<<<(int)(blocks < 1 ? 1 : blocks), 256, 0, L.stream>>>(in, count, out);
+    ++*L.launches;
+}
+
 // tetrahedra per slot
 __global__ void k_b_slot_tets(const int* __restrict__ base, const int* __restrict__ slotW, int nslots,
                               int* __restrict__ tc) {

@@ -115,6 +115,14 @@ G4D_API g4d_status g4d_triangulate(g4d_ctx* ctx, const double* xyz, int n, g4d_t
 G4D_API g4d_status g4d_triangulate_to(g4d_ctx* ctx, const double* xyz, int n, g4d_tet* out, int cap, int* ntet,
                               int* sorted_to_input, g4d_stats* stats);
 
+/* The same for float coordinates (the reference's default RealType =
+ * float, Common/Geometry.h:53-57; Point3 = float[3]): the points are widened
+ * to double on the device (exact), so the result is the triangulation of the
+ * same values. The predicates stay exact, like the reference's float build;
+ * for degenerate inputs the SoS ranks follow this library's double scaling. */
+G4D_API g4d_status g4d_triangulate_to_f32(g4d_ctx* ctx, const float* xyz, int n, g4d_tet* out, int cap,
+                                          int* ntet, int* sorted_to_input, g4d_stats* stats);
+
 /* Same on device memory (inputs already resident in HBM, output left there).
  * d_xyz: n*3 doubles on ctx's device. The tetrahedra stay in a context-owned
  * device buffer returned through *d_tets (valid until the next call). */

@@ -163,3 +163,19 @@ def test_tiny_clouds_pump_and_match(oracle):
         ref, _, _ = oracle.triangulate(pts, 32)
         g, r = _canon(oracle, tets), oracle.canonical(ref)
         assert np.array_equal(g[0], r[0]) and np.array_equal(g[1], r[1]), n
+
+
+def test_float32_points_match_the_widened_double_path(tri, oracle):
+    """g4d_triangulate_to_f32 (the reference's default float RealType): the
+    same tetrahedra and adjacency as the double path on the widened values,
+    and as the oracle."""
+    pts32 = workloads.mixed(30000, seed=12).astype(np.float32)
+    _, first = np.unique(pts32, axis=0, return_index=True)
+    pts32 = np.ascontiguousarray(pts32[np.sort(first)])
+    a, _, _ = tri.triangulate(pts32)
+    b, _, _ = tri.triangulate(pts32.astype(np.float64))
+    ga, gb = _canon(oracle, a), _canon(oracle, b)
+    assert np.array_equal(ga[0], gb[0]) and np.array_equal(ga[1], gb[1])
+    ref, _, _ = oracle.triangulate(pts32.astype(np.float64), 256)
+    r = oracle.canonical(ref)
+    assert np.array_equal(ga[0], r[0]) and np.array_equal(ga[1], r[1])
