@@ -5,7 +5,7 @@ Application.cpp:213-603):
                            [-d Distribution] [-f FacetMax] [-verbose] [-stats]
                            [-timing] [-check] [-inFile F] [-outFile F]
                            [-predThreadNum N] [-predBlockNum N] [-sort]
-                           [-proposal WEIGHTS.npy] [-device D]
+                           [-proposal WEIGHTS.npy] [-device D] [-float]
 
 Generated points lie in grid units [1, G-2] like the reference's makePoints
 (Application.cpp:316-360) and go through the gdelInit/gdelCompute facade in
@@ -17,6 +17,9 @@ point sets differ from the reference binary's for the same seed.
 -f, -predThreadNum and -predBlockNum are accepted and have no effect (no
 per-loop facet bound, no fixed exact-predicate thread pool). -proposal loads
 learned star-proposal weights (float32[9473], see Triangulator.train_proposal).
+-float rounds the points to float32 first, like the reference's default
+RealType = float build (Common/Geometry.h:53-57, file input parsed as float at
+Application.cpp:501-511); the triangulation is then that of the float values.
 """
 import sys
 import time
@@ -26,7 +29,7 @@ import numpy as np
 DISTRIBUTIONS = ("Uniform", "Gaussian", "Ball", "Sphere", "Grid")
 
 USAGE = ("Syntax: gstar4d [-n PointNum] [-g GridSize] [-s Seed] [-r Max] [-d Distribution] [-f FacetMax] "
-         "[-verbose] [-stats] [-timing] [-check] [-inFile F] [-outFile F] [-proposal W.npy] [-device D]\n"
+         "[-verbose] [-stats] [-timing] [-check] [-inFile F] [-outFile F] [-proposal W.npy] [-device D] [-float]\n"
          "Distribution: 0 - Uniform, 1 - Gaussian, 2 - Ball, 3 - Sphere, 4 - Grid")
 
 
@@ -34,12 +37,14 @@ def parse_args(argv):
     """Returns the option dict, or raises ValueError on a bad argument."""
     o = {"seed": 0, "run_num": 1, "grid": 256, "n": 100000, "dist": 0, "facet_max": -1, "verbose": False,
          "stats": False, "timing": False, "check": False, "in_file": None, "out_file": None,
-         "pred_thread_num": -1, "pred_block_num": -1, "sort": True, "proposal": None, "device": 0, "help": False}
+         "pred_thread_num": -1, "pred_block_num": -1, "sort": True, "proposal": None, "device": 0, "help": False,
+         "float": False}
     valued = {"-n": ("n", int), "-g": ("grid", int), "-r": ("run_num", int), "-s": ("seed", int),
               "-f": ("facet_max", int), "-d": ("dist", int), "-inFile": ("in_file", str),
               "-outFile": ("out_file", str), "-predThreadNum": ("pred_thread_num", int),
               "-predBlockNum": ("pred_block_num", int), "-proposal": ("proposal", str), "-device": ("device", int)}
-    flags = {"-verbose": "verbose", "-stats": "stats", "-timing": "timing", "-check": "check", "-sort": "sort"}
+    flags = {"-verbose": "verbose", "-stats": "stats", "-timing": "timing", "-check": "check", "-sort": "sort",
+             "-float": "float"}
     i = 0
     while i < len(argv):
         a = argv[i]
@@ -96,11 +101,19 @@ def make_points(n, grid, dist, seed):
     return np.ascontiguousarray(out[0][:n])
 
 
-def read_points(path):
+def as_float_values(points):
+    """Points rounded to float32 (then held as the equal doubles), duplicates
+    the rounding creates dropped (first occurrence kept)."""
+    p = np.asarray(points, dtype=np.float32).astype(np.float64)
+    _, first = np.unique(p, axis=0, return_index=True)
+    return np.ascontiguousarray(p[np.sort(first)])
+
+
+def read_points(path, as_float=False):
     """Whitespace-separated coordinates, three per point, duplicates dropped
-    (first occurrence kept)."""
+    (first occurrence kept); parsed as float32 values with as_float."""
     with open(path) as f:
-        vals = np.array(f.read().split(), dtype=np.float64)
+        vals = np.array(f.read().split(), dtype=np.float32 if as_float else np.float64).astype(np.float64)
     pts = vals[: len(vals) // 3 * 3].reshape(-1, 3)
     _, first = np.unique(pts, axis=0, return_index=True)
     return np.ascontiguousarray(pts[np.sort(first)])
@@ -167,11 +180,13 @@ def main(argv=None):
                 t.proposal_weights(weights)
             t0 = time.perf_counter()
             if o["in_file"]:
-                pts = read_points(o["in_file"])
+                pts = read_points(o["in_file"], o["float"])
                 tets, _, st = t.triangulate(pts)
                 times = (st["t_pba_ms"], st["t_star_ms"], st["t_splay_ms"], st["t_out_ms"])
             else:
                 pts = make_points(o["n"], o["grid"], o["dist"], o["seed"] + run)
+                if o["float"]:
+                    pts = as_float_values(pts)
                 work = pts.copy()
                 t.gdel_init(work)
                 times = t.gdel_compute()

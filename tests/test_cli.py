@@ -51,3 +51,17 @@ def test_ply_layout_and_adjacency_check(tmp_path):
     lines = f.read_text().splitlines()
     assert lines[0] == "ply" and "element vertex 5" in lines and "element face 6" in lines
     assert lines[lines.index("end_header") + 6] == "3 0 1 2"
+
+
+def test_float_flag_rounds_points_to_float32(tmp_path):
+    """-float: the reference's default float build reads and holds float32
+    coordinates; the points become those values (as doubles), and points the
+    rounding makes equal are dropped."""
+    assert cli.parse_args(["-float"])["float"] and not cli.parse_args([])["float"]
+    f = tmp_path / "pts.txt"
+    f.write_text("0.1 0.2 0.3\n0.10000000001 0.2 0.3\n1 2 3\n")
+    p = cli.read_points(str(f), as_float=True)
+    assert p.dtype == np.float64 and len(p) == 2
+    assert np.array_equal(p[0], np.array([0.1, 0.2, 0.3], np.float32).astype(np.float64))
+    g = cli.as_float_values(cli.make_points(2000, 64, 0, seed=1))
+    assert np.array_equal(g, g.astype(np.float32).astype(np.float64))
