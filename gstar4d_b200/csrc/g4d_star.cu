@@ -644,7 +644,9 @@ __device__ void warp_load(WS<C>& S, const Dev& D, int lane, int s, StarHdr h) {
         const int e = gh[k];
         S.hh[k] = e;
         const bool occ = (uint32_t)(e & (int)HID) != HEMPTY;
-        if (occ) ws_cache_coords(S, D, k, e & (int)HID);
+        // only link vertices are triangle vertices: the coordinates of
+        // drowned history entries are never read
+        if (occ && (e & (int)HLINK)) ws_cache_coords(S, D, k, e & (int)HID);
         const unsigned m = __ballot_sync(0xffffffffu, occ && (e & (int)HLINK) != 0);
         if (lane == 0) { S.wasLink[k >> 5] = m; S.insMask[k >> 5] = 0; }
     }
