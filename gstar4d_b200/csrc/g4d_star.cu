@@ -1027,7 +1027,7 @@ __device__ __forceinline__ const int* stage_ids(const StarView& V, int* smem, in
     return smem;
 }
 
-__global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_emit(Dev D, int count) {
+__global__ void __launch_bounds__(32 * WARPS_PER_BLOCK, 10) k_emit(Dev D, int count) {
     __shared__ int shh[WARPS_PER_BLOCK][HSLOTS];
     const int lane = threadIdx.x & 31;
     const int warps = gridDim.x * WARPS_PER_BLOCK;
@@ -1760,7 +1760,7 @@ void launch_requeue(const Launch& L, const Dev& D, int count) {
 }
 
 void launch_emit(const Launch& L, const Dev& D, int count) {
-    k_emit<<<star_blocks(count), 32 * WARPS_PER_BLOCK, 0, L.stream>>>(D, count);
+    k_emit<<<star_blocks(count, WARPS_PER_BLOCK, 10), 32 * WARPS_PER_BLOCK, 0, L.stream>>>(D, count);
     ++*L.launches;
 }
 
@@ -1799,7 +1799,7 @@ void launch_tet_count(const Launch& L, const Dev& D, int* cnt) {
 void launch_tet_write(const Launch& L, const Dev& D, const int* base, g4d_tet* tets, const int* sorted_to_input,
                       int4* face, int ntet, int2* fix) {
     cudaMemsetAsync(&D.ctr->fix_next, 0, sizeof(int), L.stream);
-    k_tet_write<<<star_blocks(D.n), 32 * WARPS_PER_BLOCK, 0, L.stream>>>(D, base, tets, sorted_to_input, face);
+    k_tet_write<<<star_blocks(D.n, WARPS_PER_BLOCK, 10), 32 * WARPS_PER_BLOCK, 0, L.stream>>>(D, base, tets, sorted_to_input, face);
     int blocks = (ntet + 255) / 256;
     if (blocks > 148 * 8) blocks = 148 * 8;
     if (blocks < 1) blocks = 1;
