@@ -8,24 +8,22 @@
 // phases are re-planned for B200:
 //   z: seeding fused with the flood. Sites are bucketed per (x,y) column by a
 //      radix sort, so each column is written once (4 B/voxel, no memset, no read).
-//   y: one CTA stages a TX x G slab (x-runs of TX voxels, one row per y) in
-//      shared memory and every thread resolves one voxel by an outward search
-//      that stops as soon as d^2 >= best (exact; 4 B read + 4 B write per voxel).
-//   x: same with G x TY contiguous rows (no transposes).
-// Sites stay encoded as voxel coordinates; they become point ids only for the
-// emitted pairs (a lookup in the column-sorted site list).
+//   y, x: one thread per line builds the lower envelope of the line's
+//      candidates and colours the line from it (O(G) per line, no transposes;
+//      k_pba_env_y / k_pba_env_x below).
+// Sites stay encoded as voxel coordinates; the pair scan turns them into point
+// ids through a voxel -> leader map written into the free second grid.
 //
 // Batches: the grids of all clouds with the same G are stacked (grid k of the
 // stack at offset k*G^3, its columns at k*G^2 in the column index), and each
 // kernel takes the stack depth K as its last grid dimension, so one launch per
 // grid size serves every cloud of that size. One cloud is a stack of depth 1.
+#include <type_traits>
+
 #include "g4d_internal.cuh"
 
 namespace g4d {
 
-#ifndef PBA_U
-#define PBA_U 2  // search distances per loop iteration in the y and x passes
-#endif
 
 template <class KeyT>
 __global__ void __launch_bounds__(128) k_pba_z(int G, const KeyT* __restrict__ ckey, const int* __restrict__ cs,
@@ -57,99 +55,6 @@ __global__ void __launch_bounds__(128) k_pba_z(int G, const KeyT* __restrict__ c
     }
 }
 
-// y pass: TX consecutive x-columns at fixed z. The slab is staged transposed
-// (one line per x, pitch G+1 so the transposing stores are conflict-free), a
-// warp resolves 32 consecutive voxels of one line (neighbouring voxels have
-// similar search lengths, so the warp stays converged), and results go
-// through a second, row-major tile so the global stores are coalesced.
-template <int TX>
-__global__ void __launch_bounds__(256) k_pba_y(int G, const uint32_t* __restrict__ in, uint32_t* __restrict__ out) {
-    extern __shared__ uint32_t smem_pba[];
-    uint32_t* lines = smem_pba;                     // [TX][G+1]
-    uint32_t* res = smem_pba + (size_t)TX * (G + 1);  // [G][TX+1]
-    const int x0 = blockIdx.x * TX;
-    const int z = blockIdx.y;
-    const size_t zoff = ((size_t)blockIdx.z * G + z) * G * G;
-    const int total = G * TX;
-    for (int k = threadIdx.x; k < total; k += blockDim.x) {
-        const int yy = k / TX, xx = k % TX;
-        lines[xx * (G + 1) + yy] = in[zoff + (size_t)yy * G + x0 + xx];
-    }
-    __syncthreads();
-    for (int k = threadIdx.x; k < total; k += blockDim.x) {
-        const int xx = k / G, y = k % G;
-        const uint32_t* line = lines + xx * (G + 1);
-        uint32_t best = line[y];
-        int bestd = best != MARKER ? (z - (int)vz(best)) * (z - (int)vz(best)) : 0x7fffffff;
-        // PBA_U distances per iteration (2 PBA_U loads in flight); the visiting
-        // order (y - d before y + d, d ascending) and the strict improvement
-        // rule are those of a one-step search, so ties resolve the same way
-        for (int d = 1; d * d < bestd; d += PBA_U) {
-            if (y - d < 0 && y + d >= G) break;
-            uint32_t c[2 * PBA_U];
-#pragma unroll
-            for (int q = 0; q < PBA_U; ++q) {
-                c[2 * q] = y - d - q >= 0 ? line[y - d - q] : MARKER;
-                c[2 * q + 1] = y + d + q < G ? line[y + d + q] : MARKER;
-            }
-#pragma unroll
-            for (int q = 0; q < 2 * PBA_U; ++q) {
-                if (c[q] == MARKER) continue;
-                const int dy = d + (q >> 1), dz = z - (int)vz(c[q]);
-                const int dd = dy * dy + dz * dz;
-                if (dd < bestd) { bestd = dd; best = c[q]; }
-            }
-        }
-        res[y * (TX + 1) + xx] = best;
-    }
-    __syncthreads();
-    for (int k = threadIdx.x; k < total; k += blockDim.x) {
-        const int yy = k / TX, xx = k % TX;
-        out[zoff + (size_t)yy * G + x0 + xx] = res[yy * (TX + 1) + xx];
-    }
-}
-
-// x pass: TY contiguous rows of G voxels at fixed z
-template <int TY>
-__global__ void __launch_bounds__(256) k_pba_x(int G, const uint32_t* __restrict__ in, uint32_t* __restrict__ out) {
-    extern __shared__ uint32_t tile[];
-    const int y0 = blockIdx.x * TY;
-    const int z = blockIdx.y;
-    const size_t base = ((size_t)blockIdx.z * G + z) * G * G + (size_t)y0 * G;
-    const int total = G * TY;
-    const uint4* in4 = reinterpret_cast<const uint4*>(in + base);
-    uint4* t4 = reinterpret_cast<uint4*>(tile);
-    for (int k = threadIdx.x; k < total / 4; k += blockDim.x) t4[k] = in4[k];
-    __syncthreads();
-    for (int k = threadIdx.x; k < total; k += blockDim.x) {
-        const int row = k / G, x = k % G;
-        const int y = y0 + row;
-        const uint32_t* line = tile + row * G;
-        uint32_t best = line[x];
-        int bestd = 0x7fffffff;
-        if (best != MARKER) {
-            const int dy = y - (int)vy(best), dz = z - (int)vz(best);
-            bestd = dy * dy + dz * dz;
-        }
-        for (int d = 1; d * d < bestd; d += PBA_U) {  // as in the y pass
-            if (x - d < 0 && x + d >= G) break;
-            uint32_t c[2 * PBA_U];
-#pragma unroll
-            for (int q = 0; q < PBA_U; ++q) {
-                c[2 * q] = x - d - q >= 0 ? line[x - d - q] : MARKER;
-                c[2 * q + 1] = x + d + q < G ? line[x + d + q] : MARKER;
-            }
-#pragma unroll
-            for (int q = 0; q < 2 * PBA_U; ++q) {
-                if (c[q] == MARKER) continue;
-                const int dx = d + (q >> 1), dy = y - (int)vy(c[q]), dz = z - (int)vz(c[q]);
-                const int dd = dx * dx + dy * dy + dz * dz;
-                if (dd < bestd) { bestd = dd; best = c[q]; }
-            }
-        }
-        out[base + k] = best;
-    }
-}
 
 
 // ---------------------------------------------------------------------------
@@ -568,48 +473,16 @@ void launch_pba_y(const Launch& L, int G, uint32_t* in, uint32_t* out) { launch_
 
 // `in` is scratch: the envelope passes keep their stacks in it
 void launch_pba_y_stack(const Launch& L, int G, int K, uint32_t* in, uint32_t* out) {
-#ifdef PBA_SEARCH
-    // two tiles of TX*G voxels: about 34 KB for G >= 256
-    const int TX = G >= 512 ? 8 : (G >= 256 ? 16 : 32);
-    const size_t sm = ((size_t)TX * (G + 1) + (size_t)G * (TX + 1)) * 4;
-    switch (TX) {
-#define G4D_Y(T)                                                                                  \
-    case T:                                                                                       \
-        cudaFuncSetAttribute(k_pba_y<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm); \
-        k_pba_y<T><<<dim3(G / T, G, K), 256, sm, L.stream>>>(G, in, out);                         \
-        break;
-        G4D_Y(8) G4D_Y(16) G4D_Y(32)
-#undef G4D_Y
-        default: break;
-    }
-#else
     if (G > 512) k_pba_env_y<true><<<dim3(G / 32, G / 4, K), dim3(32, 4), 0, L.stream>>>(G, in, out);
     else k_pba_env_y<false><<<dim3(G / 32, G / 4, K), dim3(32, 4), 0, L.stream>>>(G, in, out);
-#endif
     ++*L.launches;
 }
 
 void launch_pba_x(const Launch& L, int G, uint32_t* in, uint32_t* out) { launch_pba_x_stack(L, G, 1, in, out); }
 
 void launch_pba_x_stack(const Launch& L, int G, int K, uint32_t* in, uint32_t* out) {
-#ifdef PBA_SEARCH
-    // TY rows of G voxels: 32 KB of shared memory per block
-    const int TY = G >= 1024 ? 8 : (G >= 512 ? 16 : (G >= 256 ? 32 : (8192 / G < G ? 8192 / G : G)));
-    const size_t sm = (size_t)G * TY * 4;
-    switch (TY) {
-#define G4D_X(T)                                                                                   \
-    case T:                                                                                        \
-        cudaFuncSetAttribute(k_pba_x<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);  \
-        k_pba_x<T><<<dim3(G / T, G, K), 256, sm, L.stream>>>(G, in, out);                          \
-        break;
-        G4D_X(8) G4D_X(16) G4D_X(32) G4D_X(64) G4D_X(128) G4D_X(256)
-#undef G4D_X
-        default: break;
-    }
-#else
     if (G > 512) k_pba_env_x<true><<<dim3(G / 32, G / 4, K), dim3(32, 4), 0, L.stream>>>(G, in, out);
     else k_pba_env_x<false><<<dim3(G / 32, G / 4, K), dim3(32, 4), 0, L.stream>>>(G, in, out);
-#endif
     ++*L.launches;
 }
 
