@@ -162,17 +162,17 @@ __device__ __forceinline__ void env_line(int G, Ops& o) {
 struct EnvY {
     uint32_t* line;
     uint32_t* res;
-    size_t st;
+    int st;  // one row along y (G words; offsets within a line fit in 32 bits)
     int x, z;
     uint32_t ahead;  // input word of the next position, loaded ahead of use
     __device__ uint32_t next_in(int q) {
-        const uint32_t w = q == (int)(st - 1) ? line[(size_t)q * st] : ahead;
-        if (q > 0) ahead = line[(size_t)(q - 1) * st];
+        const uint32_t w = ahead;
+        if (q > 0) ahead = line[(q - 1) * st];
         return w;
     }
-    __device__ uint32_t at(int p) const { return line[(size_t)p * st]; }
+    __device__ uint32_t at(int p) const { return line[p * st]; }
     __device__ void put(int p, uint32_t w) const {
-        if (w != MARKER) line[(size_t)p * st] = w;
+        if (w != MARKER) line[p * st] = w;
     }
     __device__ int fin(uint32_t w) const { const int d = z - (int)vz(w); return d * d; }
     __device__ int fpk(uint32_t w) const { const int d = z - (int)(w & 1023u); return d * d; }
@@ -181,7 +181,7 @@ struct EnvY {
     __device__ uint32_t site(int p, uint32_t w) const { return enc_vox((uint32_t)x, (uint32_t)p, w & 1023u); }
     __device__ void emit(int y, uint32_t v) const {
         __syncwarp();  // one full line per warp store
-        res[(size_t)y * st] = v;
+        res[y * st] = v;
     }
 };
 
@@ -192,7 +192,7 @@ __global__ void __launch_bounds__(128) k_pba_env_y(int G, uint32_t* __restrict__
     if (x >= G || z >= G) return;
     const size_t plane = (size_t)G * G;
     const size_t off = (size_t)blockIdx.z * plane * G + (size_t)z * plane + x;
-    EnvY o{in + off, out + off, (size_t)G, x, z, 0u};
+    EnvY o{in + off, out + off, G, x, z, in[off + (size_t)(G - 1) * G]};
     env_line<WIDE>(G, o);
 }
 
