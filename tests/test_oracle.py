@@ -42,11 +42,13 @@ def test_orient4_sos_is_antisymmetric(oracle):
         assert s == d["sign"][k] * (-1) ** inv
 
 
-@pytest.mark.skipif(not os.path.isdir("/root/reference"), reason="reference sources not mounted")
 def test_orient4_sos_random_against_reference_build(oracle):
     import ctypes
-    oracle.build()
-    dev = ctypes.CDLL(os.path.join(oracle.REF_DIR, "libref_devpred.so"))
+    oracle.build()  # also builds oracle/_ref when the reference sources are mounted
+    path = os.path.join(oracle.REF_DIR, "libref_devpred.so")
+    if not os.path.exists(path):
+        pytest.skip("reference build unavailable")
+    dev = ctypes.CDLL(path)
     rng = np.random.default_rng(11)
     for _ in range(3000):
         p = rng.integers(0, 3, size=(5, 3)) / 2.0
