@@ -7,13 +7,22 @@ Application.cpp:213-603):
                            [-predThreadNum N] [-predBlockNum N] [-sort]
                            [-proposal WEIGHTS.npy] [-device D] [-float]
 
-Generated points lie in grid units [1, G-2] like the reference's makePoints
-(Application.cpp:316-360) and go through the gdelInit/gdelCompute facade in
-the Morton index space; points read with -inFile (whitespace-separated
-coordinates, duplicates dropped, Application.cpp:475-587) are scaled like
-_scalePoint (Application.cpp:589-603). The generators follow the reference's
-five distributions with this package's own seeded random numbers, so the
-point sets differ from the reference binary's for the same seed.
+Runs follow the reference's Application::doRun / _doRun (Application.cpp:100-307):
+per run a "Seed:" line, the points, the gdelInit/gdelCompute facade in the
+Morton index space, the Init / PBA / InitStar / Consistency / StarOutput /
+Total Time block (milliseconds), -check and -outFile on the Morton-sorted
+points, the seed incremented; after the runs one line appended to
+gStar4D-time.txt (and to gStar4D-count.txt with -stats) in the reference's CSV
+layout, times averaged in seconds. Generated points lie in grid units
+[1, G-2] like the reference's makePoints (Application.cpp:316-360); points read
+with -inFile are parsed as float values (the reference reads float tokens in
+both of its builds), duplicates dropped, and scaled like _scalePoint
+(Application.cpp:589-603) in place, so the scaled points are the ones
+triangulated, as in the reference. -outFile also writes the input points
+(Input-Points.asc, or Input-Scaled-Points.asc for file input). The generators
+follow the reference's five distributions with this package's own seeded
+random numbers, so the point sets differ from the reference binary's for the
+same seed.
 -f, -predThreadNum and -predBlockNum are accepted and have no effect (no
 per-loop facet bound, no fixed exact-predicate thread pool). -proposal loads
 learned star-proposal weights (float32[9473], see Triangulator.train_proposal).
@@ -109,6 +118,31 @@ def as_float_values(points):
     return np.ascontiguousarray(p[np.sort(first)])
 
 
+def read_point_file(path):
+    """The reference's readPoints (Application.cpp:475-587): whitespace-
+    separated tokens parsed as float, three per point, duplicates dropped (first
+    occurrence kept). Returns (points as float64 holding the float values, the
+    float minimum and maximum over all tokens, number of duplicates)."""
+    with open(path) as f:
+        vals = np.array(f.read().split(), dtype=np.float32)
+    mn = np.float32(vals.min()) if len(vals) else np.float32(0)
+    mx = np.float32(vals.max()) if len(vals) else np.float32(0)
+    pts = vals[: len(vals) // 3 * 3].astype(np.float64).reshape(-1, 3)
+    _, first = np.unique(pts, axis=0, return_index=True)
+    keep = np.sort(first)
+    return np.ascontiguousarray(pts[keep]), mn, mx, len(pts) - len(keep)
+
+
+def scale_points(points, grid, mn, mx):
+    """_scalePoint (Application.cpp:589-603): v -> (G - 3) (v - min) / (max -
+    min) + 1 with the float bounds (their difference taken in float), the rest
+    in double; duplicates the scaling creates are dropped."""
+    rng = np.float64(np.float32(mx) - np.float32(mn))
+    p = (float(grid) - 3.0) * (np.asarray(points, np.float64) - np.float64(mn)) / rng + 1.0
+    _, first = np.unique(p, axis=0, return_index=True)
+    return np.ascontiguousarray(p[np.sort(first)])
+
+
 def read_points(path, as_float=False):
     """Whitespace-separated coordinates, three per point, duplicates dropped
     (first occurrence kept); parsed as float32 values with as_float."""
@@ -117,6 +151,30 @@ def read_points(path, as_float=False):
     pts = vals[: len(vals) // 3 * 3].reshape(-1, 3)
     _, first = np.unique(pts, axis=0, return_index=True)
     return np.ascontiguousarray(pts[np.sort(first)])
+
+
+def write_asc(path, points):
+    """One point per line, coordinates separated by spaces, printed like the
+    reference's default stream formatting (6 significant digits)."""
+    with open(path, "w") as f:
+        for p in np.asarray(points, np.float64):
+            f.write("%g %g %g\n" % (p[0], p[1], p[2]))
+
+
+def log_lines(o, n, sums):
+    """The lines the reference appends to gStar4D-time.txt and
+    gStar4D-count.txt (Application.cpp:160-196). sums: per-stage millisecond
+    sums over the runs (init, pba, star, splay, out, total) and the insertion
+    and loop counters; times are averaged and given in seconds."""
+    runs = o["run_num"]
+    head = "GridSize,%d,Runs,%d,Points,%d,Input,%s," % (
+        o["grid"], runs, n, o["in_file"] if o["in_file"] else DISTRIBUTIONS[o["dist"]])
+    sec = lambda k: "%g" % (sums[k] / (runs * 1000.0))
+    time_line = head + ("Total Time,%s,Init Time,%s,PBA Time,%s,Star Time,%s,Splay Time,%s,Out Time,%s" % (
+        sec("total"), sec("init"), sec("pba"), sec("star"), sec("splay"), sec("out")))
+    count_line = head + "Total insertions,%d,Star insertions,%d,Splay insertions,%d,Loop number,%d" % (
+        sums["star_ins"] + sums["splay_ins"], sums["star_ins"], sums["splay_ins"], sums["loops"])
+    return time_line, count_line
 
 
 def write_ply(path, points, tets):
@@ -165,44 +223,64 @@ def main(argv=None):
         print(USAGE)
         return 1
     import gstar4d_b200
-    print("GDelaunay ... Seed: %d RunNum: %d Dist: %d Grid: %d %s" % (
-        o["seed"], o["run_num"], o["dist"], o["grid"],
-        ("Input: " + o["in_file"]) if o["in_file"] else ("Points: %d" % o["n"])))
     weights = np.load(o["proposal"]).astype(np.float32) if o["proposal"] else None
     cfg = dict(grid_size=o["grid"], do_check=int(o["check"]), log_verbose=int(o["verbose"]),
                log_stats=int(o["stats"]), log_timing=int(o["timing"]), device=o["device"],
                facet_max=o["facet_max"], pred_thread_num=o["pred_thread_num"],
                pred_block_num=o["pred_block_num"], proposal=int(weights is not None))
+    sums = dict(init=0.0, pba=0.0, star=0.0, splay=0.0, out=0.0, total=0.0, star_ins=0, splay_ins=0, loops=0)
     totals = []
+    n_used = o["n"]
     for run in range(o["run_num"]):
+        seed = o["seed"] + run
+        print("Seed: %d" % seed)
+        if o["in_file"]:
+            print("Reading from point file ...")
+            raw, mn, mx, dups = read_point_file(o["in_file"])
+            if dups:
+                print("%d duplicate points in input file!" % dups)
+            pts = scale_points(raw, o["grid"], mn, mx)
+            if o["stats"]:
+                print("Min: %g Max: %g Min-Scaled: %g Max-Scaled: %g" % (
+                    mn, mx, 1.0, (o["grid"] - 3.0) + 1.0))
+            if o["out_file"]:
+                write_asc("Input-Scaled-Points.asc", pts)
+        else:
+            pts = make_points(o["n"], o["grid"], o["dist"], seed)
+            if o["float"]:
+                pts = as_float_values(pts)
+            if o["out_file"]:
+                write_asc("Input-Points.asc", pts)
+        n_used = len(pts)
+        work = np.ascontiguousarray(pts, dtype=np.float64).copy()
         with gstar4d_b200.Triangulator(**cfg) as t:
             if weights is not None:
                 t.proposal_weights(weights)
             t0 = time.perf_counter()
-            if o["in_file"]:
-                pts = read_points(o["in_file"], o["float"])
-                tets, _, st = t.triangulate(pts)
-                times = (st["t_pba_ms"], st["t_star_ms"], st["t_splay_ms"], st["t_out_ms"])
-            else:
-                pts = make_points(o["n"], o["grid"], o["dist"], o["seed"] + run)
-                if o["float"]:
-                    pts = as_float_values(pts)
-                work = pts.copy()
-                t.gdel_init(work)
-                times = t.gdel_compute()
-                tets = t.get_tetra_from_gpu()
-                st = t.stats()
-                t.gdel_deinit()
-                pts = work  # the tetrahedra index the Morton-sorted points
-            wall = (time.perf_counter() - t0) * 1e3
-        total = sum(times)
-        totals.append(total)
-        if o["timing"] or o["verbose"]:
-            print("PBA: %.3f ms  InitStar: %.3f ms  Consistent: %.3f ms  Output: %.3f ms" % tuple(times))
+            t.gdel_init(work)  # sorted in place, like gdelInit
+            init_ms = (time.perf_counter() - t0) * 1e3
+            times = t.gdel_compute()
+            tot_ms = (time.perf_counter() - t0) * 1e3
+            tets = t.get_tetra_from_gpu() if (o["check"] or o["out_file"]) else None
+            st = t.stats()
+            t.gdel_deinit()
+        print("")
+        print("Init:        %g" % init_ms)
+        print("PBA:         %g" % times[0])
+        print("InitStar:    %g" % times[1])
+        print("Consistency: %g" % times[2])
+        print("StarOutput:  %g" % times[3])
+        print("")
+        print("Total Time:  %g" % tot_ms)
+        for k, v in zip(("init", "pba", "star", "splay", "out", "total"), (init_ms,) + tuple(times) + (tot_ms,)):
+            sums[k] += v
+        sums["star_ins"] += st["star_insertions"]
+        sums["splay_ins"] += st["splay_insertions"]
+        sums["loops"] += st["loops"]
+        totals.append(tot_ms)
         if o["stats"] or o["verbose"]:
             print("Star insertions: %d  Splay insertions: %d  Loops: %d  Tetra: %d  Exact predicates: %d" % (
-                st["star_insertions"], st["splay_insertions"], st["loops"], len(tets), st["exact_predicates"]))
-        print("Total Time: %.3f ms (call %.3f ms)" % (total, wall))
+                st["star_insertions"], st["splay_insertions"], st["loops"], st["tets"], st["exact_predicates"]))
         if o["check"]:
             bad = check_adjacency(tets)
             print("Check: stars consistent on the device; %s" % (
@@ -210,9 +288,13 @@ def main(argv=None):
             if bad:
                 return 2
         if o["out_file"]:
-            write_ply(o["out_file"], pts, tets)
-    if o["run_num"] > 1:
-        print("Average Total Time: %.3f ms" % (sum(totals) / len(totals)))
+            write_ply(o["out_file"], work, tets)  # the tetrahedra index the Morton-sorted points
+    time_line, count_line = log_lines(o, n_used, sums)
+    with open("gStar4D-time.txt", "a") as f:
+        f.write(time_line + "\n")
+    if o["stats"]:
+        with open("gStar4D-count.txt", "a") as f:
+            f.write(count_line + "\n")
     return 0
 
 

@@ -65,3 +65,30 @@ def test_float_flag_rounds_points_to_float32(tmp_path):
     assert np.array_equal(p[0], np.array([0.1, 0.2, 0.3], np.float32).astype(np.float64))
     g = cli.as_float_values(cli.make_points(2000, 64, 0, seed=1))
     assert np.array_equal(g, g.astype(np.float32).astype(np.float64))
+
+
+def test_file_input_is_read_as_float_and_scaled_like_the_reference(tmp_path):
+    """readPoints + _scalePoint (Application.cpp:475-603): float tokens, the
+    bounds over all tokens, duplicates dropped, v -> (G-3)(v-min)/(max-min)+1."""
+    f = tmp_path / "pts.txt"
+    f.write_text("0.1 2 3\n4 5 6\n0.1 2 3\n-1 0.5 7\n")
+    raw, mn, mx, dups = cli.read_point_file(str(f))
+    assert dups == 1 and len(raw) == 3
+    assert mn == np.float32(-1) and mx == np.float32(7)
+    assert raw[0, 0] == float(np.float32(0.1))
+    s = cli.scale_points(raw, 64, mn, mx)
+    assert s.min() >= 1.0 and s.max() <= 62.0
+    assert np.isclose(s[2, 0], 1.0) and np.isclose(s[2, 2], 62.0)
+
+
+def test_log_lines_follow_the_reference_layout(tmp_path):
+    o = cli.parse_args(["-g", "256", "-r", "2", "-d", "1", "-n", "1000"])
+    sums = dict(init=2.0, pba=4.0, star=6.0, splay=8.0, out=2.0, total=22.0, star_ins=30, splay_ins=5, loops=7)
+    t, c = cli.log_lines(o, 1000, sums)
+    assert t == ("GridSize,256,Runs,2,Points,1000,Input,Gaussian,Total Time,0.011,Init Time,0.001,"
+                 "PBA Time,0.002,Star Time,0.003,Splay Time,0.004,Out Time,0.001")
+    assert c == ("GridSize,256,Runs,2,Points,1000,Input,Gaussian,Total insertions,35,Star insertions,30,"
+                 "Splay insertions,5,Loop number,7")
+    p = tmp_path / "a.asc"
+    cli.write_asc(str(p), np.array([[1.5, 2.0, 1234567.0]]))
+    assert p.read_text() == "1.5 2 1.23457e+06\n"

@@ -1,0 +1,41 @@
+"""The command line end to end (generated points and -inFile) on a B200: the
+reference's output block, -check, -outFile files and the appended log lines."""
+import os
+
+import numpy as np
+import pytest
+
+from gstar4d_b200 import __main__ as cli
+
+pytestmark = pytest.mark.gpu
+
+
+def test_generated_points_run_check_and_files(tmp_path, capsys, monkeypatch):
+    monkeypatch.chdir(tmp_path)
+    rc = cli.main(["-n", "3000", "-g", "64", "-s", "3", "-r", "2", "-d", "1", "-check", "-stats",
+                   "-outFile", "mesh.ply"])
+    assert rc == 0
+    out = capsys.readouterr().out
+    assert "Seed: 3" in out and "Seed: 4" in out
+    for label in ("Init:", "PBA:", "InitStar:", "Consistency:", "StarOutput:", "Total Time:"):
+        assert out.count(label) == 2
+    assert out.count("adjacency OK") == 2
+    assert os.path.exists("mesh.ply") and os.path.exists("Input-Points.asc")
+    assert len(open("Input-Points.asc").read().splitlines()) == 3000
+    t = open("gStar4D-time.txt").read().splitlines()
+    c = open("gStar4D-count.txt").read().splitlines()
+    assert len(t) == 1 and t[0].startswith("GridSize,64,Runs,2,Points,3000,Input,Gaussian,Total Time,")
+    assert len(c) == 1 and ",Loop number," in c[0]
+
+
+def test_file_input_is_scaled_and_triangulated(tmp_path, capsys, monkeypatch):
+    monkeypatch.chdir(tmp_path)
+    pts = np.random.default_rng(5).random((2000, 3)) * 10.0 - 3.0
+    pts = np.vstack([pts, pts[:5]])  # five duplicates
+    np.savetxt("in.txt", pts)
+    rc = cli.main(["-inFile", "in.txt", "-g", "64", "-check", "-outFile", "m.ply"])
+    assert rc == 0
+    out = capsys.readouterr().out
+    assert "5 duplicate points in input file!" in out and "adjacency OK" in out
+    s = np.loadtxt("Input-Scaled-Points.asc")
+    assert len(s) == 2000 and s.min() >= 1.0 - 1e-4 and s.max() <= 62.0 + 1e-4
