@@ -13,12 +13,16 @@
 // per-star inboxes; the loop ends when no star receives a new point.
 //
 // Storage classes. The reference grows each star's triangle array on demand
-// (GDelData.cu:306-340). Here a star lives in a fixed small slot (255 history
-// points, 252 triangles, 4 KB in HBM, 16 KB of shared memory while a warp works
-// on it) that fits nearly every star; a star that outgrows it during a round is
-// left untouched, its inbox kept, and k_promote copies it to a large slot
-// (2047 points, 2044 triangles) before the large-class kernel replays the
+// (GDelData.cu:306-340). Here a star lives in a fixed small slot (127 history
+// points, 124 triangles, 2 KB in HBM, 6.7 KB of shared memory while a warp
+// works on it) that fits nearly every star; a star that outgrows it during a
+// round is left untouched, its inbox kept, and k_promote copies it to a large
+// slot (2047 points, 2044 triangles) before the large-class kernel replays the
 // round's insertions for it. lidx[s] says which class holds star s.
+//
+// Every star kernel also exists as a filter-only variant (FP64 filters only,
+// 64 registers, 32 warps/SM): a star, proof or count that meets an undecided
+// predicate is left untouched and queued for the exact variant.
 #include "g4d_internal.cuh"
 #include "g4d_predicates.cuh"
 
@@ -103,7 +107,7 @@ struct LargeStar {
     __device__ static Tri* tris(const Dev& D, int s) { return D.ltri + (size_t)D.lidx[s] * TS; }
 };
 
-// Per-warp shared-memory image of one star (7.4 KB small, so that 24 warps fit
+// Per-warp shared-memory image of one star (6.7 KB small, so that 32 warps fit
 // on an SM; 141 KB large).
 template <class C>
 struct WS {
@@ -269,11 +273,10 @@ __device__ __forceinline__ void ws_cache_coords(WS<C>& S, const Dev& D, int slot
     S.cz[cc] = p.z;
 }
 
-// membership of v in star `star`: 0 = never inserted, 1 = in the history but
-// not in the link, 2 = in the link
-// History probe of id v in `star`, 0 absent, 1 present, 2 linked. The first
-// probe of the small table is issued together with the class lookup (lidx), so
-// a small star, the common case, costs one round trip instead of two.
+// Membership of v in star `star`: 0 = never inserted, 1 = in the history but
+// not in the link, 2 = in the link. The first probe of the small table is
+// issued together with the class lookup (lidx), so a small star, the common
+// case, costs one round trip instead of two.
 struct HistProbe {
     const int* h;
     uint32_t mask, pos, e;
