@@ -2,8 +2,9 @@
 //
 // Replaces the reference's facade and host drivers (GDelaunay/GDelaunay.cpp:
 // 47-104, GDelHost.cu:136-1630): status codes instead of exit(-1), one context
-// per host thread, a CUDA stream per context, CUB for the radix sorts and scans
-// the reference did with Thrust, and one host read of a few counters per
+// per host thread, CUDA streams per context (the pipeline, containment proofs
+// beside emission, batch results to host), CUB for the radix sorts and scans
+// the reference did with Thrust, and two host reads of a few counters per
 // splaying round instead of dozens of implicit device->host reads.
 #include <cub/cub.cuh>
 

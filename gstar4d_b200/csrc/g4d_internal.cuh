@@ -3,7 +3,9 @@
 // HBM layout (n points, G^3 grid):
 //   P        double4[n]     points in Morton order (x,y,z,0): one 32-byte sector each
 //   vox      uint32[n]      voxel of each point, packed x | y<<10 | z<<20
-//   grid A/B uint32[G^3]    digital Voronoi sites, packed voxel coords, x fastest
+//   grid A   uint32[G^3]    digital Voronoi sites, packed voxel coords, x fastest
+//   grid B   uint32[G^3]    scratch of the envelope passes, then the voxel ->
+//                           leader-id map of the pair scan
 //   hh       int32[n*256]   per-star history hash: every point ever inserted in the
 //                           star (bit 31 = currently in the link), open addressing
 //   tri      uint2[n*128]   per-star link triangles, 8 bytes each (packing below)
