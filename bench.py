@@ -434,7 +434,7 @@ def main():
             "clocks": clocks,
             "gpu_launches": int(launches),
         }
-        if not args.no_cpu:
+        if not args.no_cpu and world == 1:  # the CPU baseline is an N=1 figure
             threads = os.cpu_count() or 1
             v, t, ns = cpu_run(1, threads)
             line["cpu_baseline"] = {"value": round(v, 4), "unit": "Mpts/s", "cores": threads, "kind": "port",
