@@ -234,6 +234,26 @@ __device__ __forceinline__ int pred4(double3 a, double3 b, double3 c, double3 d,
     return orient4_filter(a, b, c, d, e);
 }
 
+// The coordinate cache of a filter-only kernel holds coordinates relative to
+// the star's point (rounded once, as the filter's own differences would be),
+// so the filter needs no subtraction; an exact kernel caches absolute
+// coordinates for its big-integer fallback. Both give the exact sign or,
+// filter-only, 0 (undecided).
+// orient4(a, b, c, star, p): p against the link triangle (a, b, c)
+template <bool EXACT>
+__device__ __forceinline__ int pred_beneath(double3 a, double3 b, double3 c, double3 ps, double3 pp, int ia, int ib,
+                                            int ic, int is, int ip, const PredSink& sink, unsigned* exact) {
+    if (EXACT) return orient4(a, b, c, ps, pp, ia, ib, ic, is, ip, sink, exact);
+    return -orient4_filter_rel(a, b, c, pp);  // the star's point as the base: rows a, b, c, p swap two points
+}
+// orient4(l0, l1, l2, l3, star)
+template <bool EXACT>
+__device__ __forceinline__ int pred_cone(double3 a, double3 b, double3 c, double3 d, double3 ps, int ia, int ib,
+                                         int ic, int id, int is, const PredSink& sink, unsigned* exact) {
+    if (EXACT) return orient4(a, b, c, d, ps, ia, ib, ic, id, is, sink, exact);
+    return orient4_filter_rel(a, b, c, d);
+}
+
 // point coordinates; an out-of-range id (only possible from a corrupted star)
 // raises ERR_TOPOLOGY and reads point 0 instead of leaving the buffer
 __device__ __forceinline__ double3 gpt(const Dev& D, int id) {
@@ -263,14 +283,14 @@ __device__ __forceinline__ void cloud_range(const Dev& D, int s, int* lo, int* h
 
 // cache the coordinates of the point in `slot`
 template <class C>
-__device__ __forceinline__ void ws_cache_coords(WS<C>& S, const Dev& D, int slot, int id) {
+__device__ __forceinline__ void ws_cache_coords(WS<C>& S, const Dev& D, int slot, int id, double3 base) {
     const int c = atomicAdd(&S.ncoord, 1);
     const int cc = c < C::HM + 1 ? c : C::HM;
     S.cix[slot] = (typename C::Idx)cc;
     const double4 p = D.P[valid_id(D, id) ? id : 0];
-    S.cx[cc] = p.x;
-    S.cy[cc] = p.y;
-    S.cz[cc] = p.z;
+    S.cx[cc] = p.x - base.x;
+    S.cy[cc] = p.y - base.y;
+    S.cz[cc] = p.z - base.z;
 }
 
 // Membership of v in star `star`: 0 = never inserted, 1 = in the history but
@@ -416,8 +436,8 @@ __device__ int warp_insert(WS<C>& S, int lane, int s, double3 ps, int sp, int ge
         if (t < ntri && (S.tf[t] & 0x80)) {
             al = true;
             a = S.tv[0][t]; bb = S.tv[1][t]; c = S.tv[2][t];
-            const int sg = pred4<EXACT>(wpt(S, a), wpt(S, bb), wpt(S, c), ps, pp, wid(S, a), wid(S, bb), wid(S, c),
-                                        s, pid, sink, exact);
+            const int sg = pred_beneath<EXACT>(wpt(S, a), wpt(S, bb), wpt(S, c), ps, pp, wid(S, a), wid(S, bb),
+                                               wid(S, c), s, pid, sink, exact);
             b = sg < 0;
             und = sg == 0;
         }
@@ -455,8 +475,8 @@ __device__ int warp_insert(WS<C>& S, int lane, int s, double3 ps, int sp, int ge
             if (t < ntri && (S.tf[t] & 0x80)) {
                 al = true;
                 const int a = S.tv[0][t], bb = S.tv[1][t], c = S.tv[2][t];
-                const int sg = pred4<EXACT>(wpt(S, a), wpt(S, bb), wpt(S, c), ps, pp, wid(S, a), wid(S, bb), wid(S, c),
-                                            s, pid, sink, exact);
+                const int sg = pred_beneath<EXACT>(wpt(S, a), wpt(S, bb), wpt(S, c), ps, pp, wid(S, a), wid(S, bb),
+                                                   wid(S, c), s, pid, sink, exact);
                 b = sg < 0;
                 und = sg == 0;
             }
@@ -583,7 +603,7 @@ template <class C, bool EXACT>
 __device__ int warp_cone(WS<C>& S, int lane, int s, double3 ps, const int* l4, int gen, const PredSink& sink,
                          unsigned* exact) {
     int l[4] = {l4[0], l4[1], l4[2], l4[3]};
-    const int o = pred4<EXACT>(wpt(S, l[0]), wpt(S, l[1]), wpt(S, l[2]), wpt(S, l[3]), ps, wid(S, l[0]),
+    const int o = pred_cone<EXACT>(wpt(S, l[0]), wpt(S, l[1]), wpt(S, l[2]), wpt(S, l[3]), ps, wid(S, l[0]),
                                wid(S, l[1]), wid(S, l[2]), wid(S, l[3]), s, sink, exact);
     if (!EXACT && o == 0) return -3;
     if (o < 0) { const int t = l[0]; l[0] = l[1]; l[1] = t; }
@@ -635,7 +655,7 @@ __device__ void warp_sort_order(WS<C>& S, int lane, int n) {
 
 // Load star s (history, coordinates, triangles) into shared memory.
 template <class C>
-__device__ void warp_load(WS<C>& S, const Dev& D, int lane, int s, StarHdr h) {
+__device__ void warp_load(WS<C>& S, const Dev& D, int lane, int s, StarHdr h, double3 base) {
     using Idx = typename C::Idx;
     if (lane == 0) {
         S.ncoord = 0;
@@ -649,7 +669,7 @@ __device__ void warp_load(WS<C>& S, const Dev& D, int lane, int s, StarHdr h) {
         const bool occ = (uint32_t)(e & (int)HID) != HEMPTY;
         // only link vertices are triangle vertices: the coordinates of
         // drowned history entries are never read
-        if (occ && (e & (int)HLINK)) ws_cache_coords(S, D, k, e & (int)HID);
+        if (occ && (e & (int)HLINK)) ws_cache_coords(S, D, k, e & (int)HID, base);
         const unsigned m = __ballot_sync(0xffffffffu, occ && (e & (int)HLINK) != 0);
         if (lane == 0) { S.wasLink[k >> 5] = m; S.insMask[k >> 5] = 0; }
     }
@@ -769,6 +789,8 @@ __global__ void __launch_bounds__(32 * C::WARPS, EXACT ? C::MINB : C::MINB_FAST)
         if (lane == 0) { S.nins = 0; S.nhist = 0; S.ntri = 0; S.nfree = 0; S.ncoord = 0; }
         __syncwarp();
         const double3 ps = gpt(D, s);
+        const double3 base = EXACT ? make_double3(0.0, 0.0, 0.0) : ps;  // of the coordinate cache
+        const double3 rb = EXACT ? ps : make_double3(0.0, 0.0, 0.0);    // cached coordinate -> relative
         // candidates from the bucket
         const int bc = min(D.bucketCount[s], BUCKET_CAP);
         for (int k = lane; k < bc; k += 32) {
@@ -828,9 +850,10 @@ __global__ void __launch_bounds__(32 * C::WARPS, EXACT ? C::MINB : C::MINB_FAST)
         for (int i = lane; i < nins; i += 32) {
             const int slot = S.order[i];
             const int id = S.hh[slot] & (int)HID;
-            ws_cache_coords(S, D, slot, id);
+            ws_cache_coords(S, D, slot, id, base);
+            // the same rounded differences either way
             const double3 p = wpt(S, slot);
-            const double dx = p.x - ps.x, dy = p.y - ps.y, dz = p.z - ps.z;
+            const double dx = p.x - rb.x, dy = p.y - rb.y, dz = p.z - rb.z;
             S.okey[i] = (float)(dx * dx + dy * dy + dz * dz);
             atomicOr(&S.insMask[slot >> 5], 1u << (slot & 31));
         }
@@ -909,8 +932,9 @@ __global__ void __launch_bounds__(32 * C::WARPS, EXACT ? C::MINB : C::MINB_FAST)
         const int s = list[w];
         if (s < 0) continue;  // moved to the large class's list (k_reroute)
         const StarHdr h = D.hdr[s];
-        warp_load(S, D, lane, s, h);
         const double3 ps = gpt(D, s);
+        const double3 base = EXACT ? make_double3(0.0, 0.0, 0.0) : ps;  // of the coordinate cache
+        warp_load(S, D, lane, s, h, base);
         const int ic = min(D.inboxCount[s], INBOX_CAP);
         int* box = D.inbox + (size_t)s * INBOX_CAP;
         for (int k = lane; k < ic; k += 32) {
@@ -922,7 +946,7 @@ __global__ void __launch_bounds__(32 * C::WARPS, EXACT ? C::MINB : C::MINB_FAST)
             if (fresh) {
                 const int pos = atomicAdd(&S.nins, 1);
                 S.order[pos < C::HM ? pos : C::HM] = (typename C::Slot)slot;
-                ws_cache_coords(S, D, slot, v);
+                ws_cache_coords(S, D, slot, v, base);
                 atomicOr(&S.insMask[slot >> 5], 1u << (slot & 31));
             }
         }
