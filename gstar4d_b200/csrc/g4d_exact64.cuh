@@ -108,7 +108,9 @@ G4D_HD int orient4_sign(const int64_t (*X)[3]) {
     for (int r = 0; r < 4; ++r)
         for (int c = 0; c < 3; ++c) D[r][c] = X[r][c] - X[4][c];
     uint64_t m2[4][4][2];
+#pragma unroll 1
     for (int i = 0; i < 4; ++i)
+#pragma unroll 1
         for (int j = i + 1; j < 4; ++j) {
             uint64_t p[2], q[2];
             smul(D[i][0], D[j][1], p);
@@ -120,12 +122,14 @@ G4D_HD int orient4_sign(const int64_t (*X)[3]) {
         }
     const int tri[4][3] = {{1, 2, 3}, {0, 2, 3}, {0, 1, 3}, {0, 1, 2}};
     uint64_t det[5] = {0, 0, 0, 0, 0};
+#pragma unroll 1
     for (int r = 0; r < 4; ++r) {
         const int i = tri[r][0], j = tri[r][1], k = tri[r][2];
         // m3 = Dz_i m2[j][k] - Dz_j m2[i][k] + Dz_k m2[i][j]
         uint64_t m3[3] = {0, 0, 0};
         const int rows[3] = {i, j, k};
         const int pr[3][2] = {{j, k}, {i, k}, {i, j}};
+#pragma unroll 1
         for (int t = 0; t < 3; ++t) {
             const int64_t z = D[rows[t]][2];
             uint64_t m[2] = {m2[pr[t][0]][pr[t][1]][0], m2[pr[t][0]][pr[t][1]][1]};
@@ -142,6 +146,7 @@ G4D_HD int orient4_sign(const int64_t (*X)[3]) {
         }
         // L = Dx^2 + Dy^2 + Dz^2
         uint64_t L[2] = {0, 0};
+#pragma unroll 1
         for (int c = 0; c < 3; ++c) {
             const uint64_t a = absu(D[r][c]);
             uint64_t sq[2];
