@@ -1152,7 +1152,7 @@ __global__ void k_requeue(Dev D, int count) {
 // the queued items (count read on the device), or over every item when the
 // queue overflowed (repeating a proof only repeats deduplicated requests).
 template <bool EXACT>
-__global__ void __launch_bounds__(32 * WARPS_PER_BLOCK, EXACT ? 1 : PROOF_BLOCKS) k_proof(Dev D, int count) {
+__global__ void __launch_bounds__(32 * WARPS_PER_BLOCK, EXACT ? 4 : PROOF_BLOCKS) k_proof(Dev D, int count) {
     __shared__ int shh[WARPS_PER_BLOCK][HSLOTS];
     const int lane = threadIdx.x & 31;
     const PredSink sink = sink_of(D);
@@ -1803,7 +1803,7 @@ void launch_proof(const Launch& L, const Dev& D, int count) {
     // read on the device, so no host round trip), then the queue is emptied
     // for the star kernels
     k_proof<false><<<star_blocks(count), 32 * WARPS_PER_BLOCK, 0, L.stream>>>(D, count);
-    k_proof<true><<<star_blocks(count, WARPS_PER_BLOCK, 2), 32 * WARPS_PER_BLOCK, 0, L.stream>>>(D, count);
+    k_proof<true><<<star_blocks(count, WARPS_PER_BLOCK, 4), 32 * WARPS_PER_BLOCK, 0, L.stream>>>(D, count);
     cudaMemsetAsync(&D.ctr->exact_next, 0, sizeof(int), L.stream);
     *L.launches += 2;
 }
