@@ -104,11 +104,25 @@ g4d_status fail(g4d_ctx* c, g4d_status s, const char* fmt, ...) {
     return s;
 }
 
+// A failed call is reported and its (non-sticky) error cleared, so that it
+// does not resurface in a later call on the same thread.
 #define CK(call)                                                                                     \
     do {                                                                                             \
         cudaError_t e_ = (call);                                                                     \
-        if (e_ != cudaSuccess) return fail(ctx, e_ == cudaErrorMemoryAllocation ? G4D_ERR_NOMEM : G4D_ERR_CUDA, \
-                                           "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+        if (e_ != cudaSuccess) {                                                                     \
+            (void)cudaGetLastError();                                                                \
+            return fail(ctx, e_ == cudaErrorMemoryAllocation ? G4D_ERR_NOMEM : G4D_ERR_CUDA,         \
+                        "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__);         \
+        }                                                                                            \
+    } while (0)
+
+// Wait for a stream, then surface any kernel launch error since the last
+// check: a launch that failed (configuration, resources) is reported only by
+// cudaGetLastError, not by the later calls.
+#define CK_SYNC(stream)                     \
+    do {                                    \
+        CK(cudaStreamSynchronize(stream));  \
+        CK(cudaGetLastError());             \
     } while (0)
 
 int auto_grid(int n) {
@@ -178,7 +192,7 @@ g4d_status grow_large(g4d_ctx* ctx, Dev& D, int used, int need) {
         CK(cudaMemcpyAsync(nh, ctx->b[B_LHH].p, hb * used, cudaMemcpyDeviceToDevice, ctx->stream));
         CK(cudaMemcpyAsync(nt, ctx->b[B_LTRI].p, tb * used, cudaMemcpyDeviceToDevice, ctx->stream));
     }
-    CK(cudaStreamSynchronize(ctx->stream));
+    CK_SYNC(ctx->stream);
     ctx->b[B_LHH].release();
     ctx->b[B_LTRI].release();
     ctx->b[B_WLINSL].release();
@@ -311,7 +325,7 @@ g4d_status grow_ovf(g4d_ctx* ctx, Dev& D, int keep, size_t need) {
     CK(cudaMalloc(&a, sizeof(int2) * need));
     CK(cudaMalloc(&b, sizeof(int2) * need));
     if (keep > 0) CK(cudaMemcpyAsync(a, D.ovf, sizeof(int2) * keep, cudaMemcpyDeviceToDevice, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    CK_SYNC(ctx->stream);
     ctx->b[B_OVF].release();
     ctx->b[B_OVF2].release();
     ctx->b[B_OVF].p = a; ctx->b[B_OVF].cap = sizeof(int2) * need;
@@ -327,7 +341,7 @@ g4d_status grow_ovf(g4d_ctx* ctx, Dev& D, int keep, size_t need) {
 g4d_status worksets_fit(g4d_ctx* ctx, Dev& D, int attempt, bool* again) {
     Counters h{};
     CK(cudaMemcpyAsync(&h, D.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    CK_SYNC(ctx->stream);
     *again = false;
     if (h.ovf_next <= D.ovfCap) return G4D_OK;
     if (attempt >= 2) return fail(ctx, G4D_ERR_CAPACITY, "overflow request list capacity exceeded");
@@ -337,7 +351,7 @@ g4d_status worksets_fit(g4d_ctx* ctx, Dev& D, int attempt, bool* again) {
     CK(cudaMemsetAsync(&D.ctr->proposed, 0, sizeof(int), ctx->stream));
     h.err &= ~(unsigned)ERR_OVFCAP;
     CK(cudaMemcpyAsync(&D.ctr->err, &h.err, sizeof(unsigned), cudaMemcpyHostToDevice, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    CK_SYNC(ctx->stream);
     *again = true;
     return G4D_OK;
 }
@@ -353,7 +367,7 @@ g4d_status run_splay(g4d_ctx* ctx, Dev& D) {
     Counters* dctr = D.ctr;
     auto read = [&]() -> g4d_status {
         CK(cudaMemcpyAsync(&h, dctr, sizeof(Counters), cudaMemcpyDeviceToHost, ctx->stream));
-        CK(cudaStreamSynchronize(ctx->stream));
+        CK_SYNC(ctx->stream);
         return check_err(ctx, h.err);
     };
     // initial stars: filter-only, then the exact kernel for the stars it left,
@@ -402,7 +416,7 @@ g4d_status run_splay(g4d_ctx* ctx, Dev& D) {
             if (emitCount) launch_emit(L, D, emitCount);
             if (drownCount) CK(cudaStreamWaitEvent(ctx->stream, ctx->join, 0));
             CK(cudaMemcpyAsync(&h, dctr, sizeof(Counters), cudaMemcpyDeviceToHost, ctx->stream));
-            CK(cudaStreamSynchronize(ctx->stream));
+            CK_SYNC(ctx->stream);
             if (!(h.err & ERR_OVFCAP) || attempt >= 3) break;
             st = grow_ovf(ctx, D, ovfCount, 2 * (size_t)h.ovf_next + (size_t)D.n);
             if (st) return st;
@@ -435,7 +449,7 @@ g4d_status run_splay(g4d_ctx* ctx, Dev& D) {
             D.anyLarge = 1;
             launch_star_insert_large(L, D, D.wlPromote, h.promote_count);
             CK(cudaMemcpyAsync(&h, dctr, sizeof(Counters), cudaMemcpyDeviceToHost, ctx->stream));
-            CK(cudaStreamSynchronize(ctx->stream));
+            CK_SYNC(ctx->stream);
             st = check_err(ctx, h.err);
             if (st) return st;
         }
@@ -463,7 +477,7 @@ g4d_status run_splay(g4d_ctx* ctx, Dev& D) {
         launch_check(L, D, bad);
         unsigned long long hb = 0;
         CK(cudaMemcpyAsync(&hb, bad, 8, cudaMemcpyDeviceToHost, ctx->stream));
-        CK(cudaStreamSynchronize(ctx->stream));
+        CK_SYNC(ctx->stream);
         if (hb) return fail(ctx, G4D_ERR_INTERNAL, "stars are not consistent (%llu missing triangles)", hb);
     }
     return G4D_OK;
@@ -485,7 +499,7 @@ g4d_status run_extract(g4d_ctx* ctx, const Dev& D, const int* sorted_to_input) {
     ++ctx->launches;
     int ntet = 0;
     CK(cudaMemcpyAsync(&ntet, base + n, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    CK_SYNC(ctx->stream);
     CK(ctx->b[B_TETS].ensure(sizeof(g4d_tet) * (size_t)std::max(ntet, 1)));
     // at most one queued link per (tetrahedron, vertex slot)
     CK(ctx->b[B_FIX].ensure(sizeof(int2) * 4 * (size_t)std::max(ntet, 1)));
@@ -496,7 +510,7 @@ g4d_status run_extract(g4d_ctx* ctx, const Dev& D, const int* sorted_to_input) {
     cudaEventRecord(ctx->ev[5], ctx->stream);
     Counters h{};
     CK(cudaMemcpyAsync(&h, D.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    CK_SYNC(ctx->stream);
     g4d_status st = check_err(ctx, h.err);
     if (st) return st;
     ctx->ntet = ntet;
@@ -537,7 +551,7 @@ g4d_status run_ring(g4d_ctx* ctx, const Dev& D, bool labels) {
     // grid units per coordinate unit, as in the scaling of the points
     unsigned long long mm[2] = {0, 0};
     CK(cudaMemcpyAsync(mm, ctx->b[B_MM].p, sizeof(mm), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    CK_SYNC(ctx->stream);
     const double range = dkey_inv_host(mm[1]) - dkey_inv_host(mm[0]);
     Ring R;
     R.grid = ctx->b[B_GA].as<uint32_t>();
@@ -553,7 +567,7 @@ g4d_status run_ring(g4d_ctx* ctx, const Dev& D, bool labels) {
     if (labels) launch_ring_labels(L, D, R.pair, R.rows, R.cap, R.y);
     MlpAux h{};
     CK(cudaMemcpyAsync(&h, aux, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    CK_SYNC(ctx->stream);
     ctx->ring_rows = std::min(h.rows, R.cap);
     return G4D_OK;
 }
@@ -685,8 +699,8 @@ g4d_status reserve_out(g4d_ctx* ctx, size_t used, size_t need) {
     void* np = nullptr;
     CK(cudaMalloc(&np, want));
     if (used && o.p) CK(cudaMemcpyAsync(np, o.p, used * sizeof(g4d_tet), cudaMemcpyDeviceToDevice, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-    if (ctx->copy_stream) CK(cudaStreamSynchronize(ctx->copy_stream));  // host copies out of the old buffer
+    CK_SYNC(ctx->stream);
+    if (ctx->copy_stream) CK_SYNC(ctx->copy_stream);  // host copies out of the old buffer
     o.release();
     o.p = np;
     o.cap = want;
@@ -834,7 +848,7 @@ g4d_status run_wave(g4d_ctx* ctx, const double* d_xyz, const int64_t* offs, cons
     launch_b_slot_tets(L, ctx->b[B_BASE].as<int>(), d_slotW, ns, d_tc);
     std::vector<int> tc(ns);
     CK(cudaMemcpyAsync(tc.data(), d_tc, sizeof(int) * ns, cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    CK_SYNC(ctx->stream);
     std::vector<int> pos_of(ns);  // slot -> position of its cloud in the list
     {
         std::vector<std::pair<int, int>> lp(ns);
@@ -933,7 +947,7 @@ g4d_status pick_batch_grids(g4d_ctx* ctx, const double* d_xyz, const int64_t* of
     launch_b_occupancy(L, d_xyz, d_offs, nclouds, d_occ);
     std::vector<int> occ(nclouds);
     CK(cudaMemcpyAsync(occ.data(), d_occ, sizeof(int) * nclouds, cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    CK_SYNC(ctx->stream);
     std::vector<int> key(nclouds);
     std::map<int, std::vector<int>> pending;
     for (int c = 0; c < nclouds; ++c) {
@@ -1175,7 +1189,7 @@ g4d_status g4d_triangulate_device(g4d_ctx* ctx, const double* d_xyz, int n, cons
         launch_b_occupancy(L, d_xyz, d_offs, 1, d_occ);
         int occ = 0;
         CK(cudaMemcpyAsync(&occ, d_occ, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-        CK(cudaStreamSynchronize(ctx->stream));
+        CK_SYNC(ctx->stream);
         const auto it = ctx->tuned.find(tune_key(n, class_of(occ, n)));
         if (it != ctx->tuned.end()) ctx->next_grid = it->second;
     }
@@ -1211,7 +1225,7 @@ g4d_status g4d_triangulate_to(g4d_ctx* ctx, const double* xyz, int n, g4d_tet* o
     if (sorted_to_input)
         CK(cudaMemcpyAsync(sorted_to_input, ctx->b[B_ORDER].p, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost,
                            ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    CK_SYNC(ctx->stream);
     if (stats) *stats = ctx->stats;
     return G4D_OK;
 }
@@ -1247,7 +1261,7 @@ g4d_status g4d_triangulate_to_f32(g4d_ctx* ctx, const float* xyz, int n, g4d_tet
     if (sorted_to_input)
         CK(cudaMemcpyAsync(sorted_to_input, ctx->b[B_ORDER].p, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost,
                            ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    CK_SYNC(ctx->stream);
     if (stats) *stats = ctx->stats;
     return G4D_OK;
 }
@@ -1262,7 +1276,7 @@ g4d_status g4d_triangulate(g4d_ctx* ctx, const double* xyz, int n, g4d_tet** tet
     g4d_tet* out = (g4d_tet*)malloc(sizeof(g4d_tet) * (size_t)std::max(nt, 1));
     if (!out) return fail(ctx, G4D_ERR_NOMEM, "host allocation of %d tetrahedra failed", nt);
     CK(cudaMemcpyAsync(out, ctx->b[B_TETS].p, sizeof(g4d_tet) * (size_t)nt, cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    CK_SYNC(ctx->stream);
     *tets = out;
     *ntet = nt;
     return G4D_OK;
@@ -1291,7 +1305,7 @@ g4d_status g4d_gdel_init(g4d_ctx* ctx, double* points, double* scaled, int n) {
     // like PointData::init (GDelData.cu:125-130): hand back the sorted order
     std::vector<int> order(n);
     CK(cudaMemcpyAsync(order.data(), ctx->b[B_ORDER].p, sizeof(int) * n, cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    CK_SYNC(ctx->stream);
     Counters h{};
     CK(cudaMemcpy(&h, ctx->b[B_CTR].p, sizeof(Counters), cudaMemcpyDeviceToHost));
     st = check_err(ctx, h.err);
@@ -1321,7 +1335,7 @@ g4d_status g4d_gdel_compute(g4d_ctx* ctx, double* t_pba, double* t_star, double*
     ctx->host_tets.resize((size_t)ctx->ntet);
     CK(cudaMemcpyAsync(ctx->host_tets.data(), ctx->b[B_TETS].p, sizeof(g4d_tet) * (size_t)ctx->ntet,
                        cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    CK_SYNC(ctx->stream);
     return G4D_OK;
 }
 
@@ -1372,7 +1386,7 @@ g4d_status g4d_triangulate_batch(g4d_ctx* ctx, const double* xyz, const int64_t*
     CK(cudaMemcpyAsync(out, ctx->b[B_BOUT].p, sizeof(g4d_tet) * ntet, cudaMemcpyDeviceToHost, ctx->stream));
     offs[0] = 0;
     for (int c = 0; c < nclouds; ++c) offs[c + 1] = offs[c] + counts[c];
-    CK(cudaStreamSynchronize(ctx->stream));
+    CK_SYNC(ctx->stream);
     *tets = out;
     *tet_offsets = offs;
     acc.t_total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -1398,7 +1412,7 @@ g4d_status g4d_triangulate_batch_to(g4d_ctx* ctx, const double* xyz, const int64
     g4d_stats acc{};
     HostSink sink{out, (size_t)cap, true};
     g4d_status st = run_batch(ctx, ctx->b[B_XYZ].as<double>(), cloud_offsets, nclouds, counts, &nt, &acc, &sink);
-    CK(cudaStreamSynchronize(ctx->copy_stream));
+    CK_SYNC(ctx->copy_stream);
     if (st) return st;
     tet_offsets[0] = 0;
     for (int c = 0; c < nclouds; ++c) tet_offsets[c + 1] = tet_offsets[c] + counts[c];
@@ -1451,7 +1465,7 @@ g4d_status g4d_eval_predicates(g4d_ctx* ctx, int kind, const double* pts, const 
     unsigned herr = 0;
     CK(cudaMemcpyAsync(out, dout, (size_t)count, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaMemcpyAsync(&herr, derr, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    CK_SYNC(ctx->stream);
     cudaFree(dp);
     cudaFree(dout);
     cudaFree(derr);
@@ -1481,7 +1495,7 @@ g4d_status g4d_voronoi(g4d_ctx* ctx, const double* xyz, int n, int grid, uint32_
     launch_pba_y(L, grid, ctx->b[B_GA].as<uint32_t>(), ctx->b[B_GB].as<uint32_t>());
     launch_pba_x(L, grid, ctx->b[B_GB].as<uint32_t>(), ctx->b[B_GA].as<uint32_t>());
     CK(cudaMemcpyAsync(sites, ctx->b[B_GA].p, sizeof(uint32_t) * G3, cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    CK_SYNC(ctx->stream);
     return G4D_OK;
 }
 
@@ -1566,13 +1580,13 @@ g4d_status g4d_proposal_train(g4d_ctx* ctx, const double* xyz, int n, int epochs
         }
         MlpAux h{};
         CK(cudaMemcpyAsync(&h, aux, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
-        CK(cudaStreamSynchronize(ctx->stream));
+        CK_SYNC(ctx->stream);
         if (h.err) return fail(ctx, G4D_ERR_INTERNAL, "tensor-core training kernel timed out waiting (0x%x)", h.err);
         last = M ? h.loss / (float)M : 0.f;
     }
     CK(cudaMemcpyAsync(ctx->mlp.data(), ctx->b[B_MLP_P].p, sizeof(float) * MLP_NPARAMS, cudaMemcpyDeviceToHost,
                        ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    CK_SYNC(ctx->stream);
     if (loss_out) *loss_out = last;
     return G4D_OK;
 }
@@ -1586,7 +1600,7 @@ g4d_status g4d_proposal_weights(g4d_ctx* ctx, float* w, int count, int set) {
         ctx->mlp.assign(w, w + MLP_NPARAMS);
         g4d_status st = mlp_upload(ctx);
         if (st) return st;
-        CK(cudaStreamSynchronize(ctx->stream));
+        CK_SYNC(ctx->stream);
         return G4D_OK;
     }
     if (!ctx->has_model) return fail(ctx, G4D_ERR_ARG, "no proposal model (train or set one first)");
@@ -1616,7 +1630,7 @@ g4d_status g4d_mlp_grad(g4d_ctx* ctx, const uint16_t* x, const float* y, int m, 
     MlpAux h{};
     CK(cudaMemcpyAsync(grads, ctx->b[B_DIAG_G].p, sizeof(float) * MLP_NPARAMS, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaMemcpyAsync(&h, aux, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    CK_SYNC(ctx->stream);
     if (h.err) return fail(ctx, G4D_ERR_INTERNAL, "tensor-core training kernel timed out waiting (0x%x)", h.err);
     if (loss) *loss = h.loss / (float)m;
     return G4D_OK;
@@ -1640,7 +1654,7 @@ g4d_status g4d_mlp_infer(g4d_ctx* ctx, const uint16_t* x, int m, const float* pa
     MlpAux h{};
     CK(cudaMemcpyAsync(logits, ctx->b[B_DIAG_Y].p, sizeof(float) * (size_t)m, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaMemcpyAsync(&h, aux, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    CK_SYNC(ctx->stream);
     if (h.err) return fail(ctx, G4D_ERR_INTERNAL, "tensor-core inference kernel timed out waiting (0x%x)", h.err);
     return G4D_OK;
 }

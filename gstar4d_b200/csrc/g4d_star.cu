@@ -1568,10 +1568,10 @@ __device__ __forceinline__ void write_star(const Dev& D, const int* base, g4d_te
 }
 
 // tetrahedra owned by small star s (a warp), one neighbour per lane: the kept
-// triangles are listed by rank, then lane k finds neighbour k&3 of tetrahedron
-// k>>2 (about 27 lookups per star, so most lanes work at once and a star costs
-// about one remote lookup of latency instead of four), then each lane writes
-// whole tetrahedra. buf: 128 B ranks, 128 B kept list, 4 ints per kept triangle.
+// triangles are listed by rank, then lane k finds the neighbour across face
+// k%3 of kept triangle k/3 (the faces that contain the owner; the face
+// opposite it is k_tet_face3's), then each lane writes whole tetrahedra.
+// buf: 128 B ranks, 128 B kept list, 3 ints per kept triangle.
 __device__ __forceinline__ void write_star_small(const Dev& D, const int* base, g4d_tet* tets,
                                                  const int* sorted_to_input, int4* face, int s, int ntri,
                                                  const int* ids, const uint2* gt, uint8_t* buf, int lane) {
@@ -1594,7 +1594,6 @@ __device__ __forceinline__ void write_star_small(const Dev& D, const int* base, 
         const int r3 = k / 3, f = k - 3 * r3;
         const uint2 T = gt[kt[r3]];
         const int s0 = SmallStar::tv(T, 0), s1 = SmallStar::tv(T, 1), s2 = SmallStar::tv(T, 2);
-        const int v0 = ids[s0] & (int)HID, v1 = ids[s1] & (int)HID, v2 = ids[s2] & (int)HID;
         // across the face (s, v[f+1], v[f+2]): the adjacent link triangle
         const int oi = SmallStar::to(T, f);
         const uint2 N = gt[oi];
