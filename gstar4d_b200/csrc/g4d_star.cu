@@ -1054,7 +1054,7 @@ __device__ __forceinline__ const int* stage_ids(const StarView& V, int* smem, in
     return smem;
 }
 
-__global__ void __launch_bounds__(32 * WARPS_PER_BLOCK, 10) k_emit(Dev D, int count) {
+__global__ void __launch_bounds__(32 * WARPS_PER_BLOCK, 16) k_emit(Dev D, int count) {
     __shared__ int shh[WARPS_PER_BLOCK][HSLOTS];
     const int lane = threadIdx.x & 31;
     const int warps = gridDim.x * WARPS_PER_BLOCK;
@@ -1786,7 +1786,7 @@ void launch_requeue(const Launch& L, const Dev& D, int count) {
 }
 
 void launch_emit(const Launch& L, const Dev& D, int count) {
-    k_emit<<<star_blocks(count, WARPS_PER_BLOCK, 10), 32 * WARPS_PER_BLOCK, 0, L.stream>>>(D, count);
+    k_emit<<<star_blocks(count, WARPS_PER_BLOCK, 16), 32 * WARPS_PER_BLOCK, 0, L.stream>>>(D, count);
     ++*L.launches;
 }
 
