@@ -19,10 +19,10 @@ with -inFile are parsed as float values (the reference reads float tokens in
 both of its builds), duplicates dropped, and scaled like _scalePoint
 (Application.cpp:589-603) in place, so the scaled points are the ones
 triangulated, as in the reference. -outFile also writes the input points
-(Input-Points.asc, or Input-Scaled-Points.asc for file input). The generators
-follow the reference's five distributions with this package's own seeded
-random numbers, so the point sets differ from the reference binary's for the
-same seed.
+(Input-Points.asc, or Input-Scaled-Points.asc for file input). Generated
+points are the reference's own: its makePoints and KISS generator (DtRandom,
+64-bit `unsigned long` as on Linux) restated in C++ (g4d_make_points), so
+`-n -g -d -s` give the same point sets as the reference binary built on Linux.
 -f, -predThreadNum and -predBlockNum are accepted and have no effect (no
 per-loop facet bound, no fixed exact-predicate thread pool). -proposal loads
 learned star-proposal weights (float32[9473], see Triangulator.train_proposal).
@@ -79,35 +79,11 @@ def parse_args(argv):
 
 
 def make_points(n, grid, dist, seed):
-    """n distinct points in grid units [1, G-2] for the five distributions."""
-    rng = np.random.default_rng(seed)
-    lo, hi = 1.0, float(grid - 2)
-    mid, half = (lo + hi) / 2.0, (hi - lo) / 2.0
-    out, have = [], 0
-    while have < n:
-        m = max(2 * (n - have), 1024)
-        if dist == 0:      # uniform in the cube
-            p = lo + (hi - lo) * rng.random((m, 3))
-        elif dist == 1:    # Gaussian about the centre, kept inside the cube
-            p = rng.normal(mid, half / 6.0, (m, 3))
-            p = p[np.all((p >= lo) & (p <= hi), axis=1)]
-        elif dist == 2:    # uniform in the ball
-            d = rng.normal(size=(m, 3))
-            d /= np.linalg.norm(d, axis=1)[:, None]
-            p = mid + half * d * np.cbrt(rng.random(m))[:, None]
-        elif dist == 3:    # on the sphere
-            d = rng.normal(size=(m, 3))
-            d /= np.linalg.norm(d, axis=1)[:, None]
-            p = mid + half * d
-        else:              # integer grid positions
-            p = np.floor(lo + (hi - lo + 1) * rng.random((m, 3)))
-            p = np.minimum(p, hi)
-        out.append(p)
-        allp = np.concatenate(out)
-        _, first = np.unique(allp, axis=0, return_index=True)
-        out = [allp[np.sort(first)]]
-        have = len(out[0])
-    return np.ascontiguousarray(out[0][:n])
+    """The reference's generated points for -n -g -d -s (Application::makePoints
+    with DtRandom's KISS numbers, restated in C++ as g4d_make_points): n
+    distinct float values in grid units [1, G-2], as float64."""
+    from gstar4d_b200 import api
+    return api.make_points(n, grid, dist, seed)
 
 
 def as_float_values(points):

@@ -38,11 +38,19 @@ class OraStats(ctypes.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+def reference_root():
+    """Where the reference sources are mounted: $REF_ROOT, else the container's
+    default mount; None when absent (e.g. on the GPU host)."""
+    root = os.environ.get("REF_ROOT", "/root/reference")
+    return root if os.path.isdir(os.path.join(root, "GDelaunay")) else None
+
+
 def build():
     """Builds liboracle.so (and oracle/_ref when the reference is mounted)."""
     subprocess.check_call(["make", "-s", "-C", HERE])
-    if os.path.isdir("/root/reference"):
-        subprocess.check_call(["make", "-s", "-C", HERE, "ref"])
+    root = reference_root()
+    if root:
+        subprocess.check_call(["make", "-s", "-C", HERE, "ref", "REF_ROOT=" + root])
 
 
 def lib():
