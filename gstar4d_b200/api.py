@@ -38,7 +38,7 @@ class Config(ctypes.Structure):
                 ("log_verbose", ctypes.c_int), ("log_stats", ctypes.c_int), ("log_timing", ctypes.c_int),
                 ("do_check", ctypes.c_int), ("pred_thread_num", ctypes.c_int), ("pred_block_num", ctypes.c_int),
                 ("do_sorting", ctypes.c_int), ("device", ctypes.c_int), ("index_space", ctypes.c_int),
-                ("proposal", ctypes.c_int)]
+                ("proposal", ctypes.c_int), ("max_splay_loops", ctypes.c_int)]
 
 
 class Stats(ctypes.Structure):
@@ -64,7 +64,7 @@ EXPORTS = ["g4d_default_config", "g4d_create", "g4d_destroy", "g4d_last_error", 
            "g4d_gdel_compute", "g4d_get_tetra", "g4d_gdel_deinit", "g4d_get_stats", "g4d_triangulate_batch",
            "g4d_triangulate_batch_to", "g4d_triangulate_batch_device", "g4d_stream",
            "g4d_eval_predicates", "g4d_voronoi", "g4d_voronoi_noalloc", "g4d_proposal_train",
-           "g4d_proposal_weights", "g4d_mlp_grad", "g4d_mlp_infer", "g4d_free"]
+           "g4d_proposal_weights", "g4d_mlp_grad", "g4d_mlp_infer", "g4d_mlp_wait_probe", "g4d_make_points", "g4d_free"]
 
 MLP_PARAMS = 9473
 
@@ -108,6 +108,8 @@ def load():
     L.g4d_proposal_weights.argtypes = [vp, vp, ip, ip]
     L.g4d_mlp_grad.argtypes = [vp, vp, vp, ip, vp, vp, fp]
     L.g4d_mlp_infer.argtypes = [vp, vp, ip, vp, vp]
+    L.g4d_mlp_wait_probe.argtypes = [vp, ip]
+    L.g4d_make_points.argtypes = [ip, ip, ip, ip, vp]
     L.g4d_stream.argtypes = [vp]
     L.g4d_stream.restype = vp
     L.g4d_free.argtypes = [vp]
@@ -274,6 +276,12 @@ class Triangulator:
         self._check(self._lib.g4d_mlp_infer(self._h, _ptr(x), len(x), _ptr(p), _ptr(out)))
         return out
 
+    def mlp_wait_probe(self, limit):
+        """Runs the tensor-core kernels' bounded wait on a phase nothing
+        completes (g4d_mlp_wait_probe); raises G4DError (status 3) when it ran
+        out, as it must."""
+        self._check(self._lib.g4d_mlp_wait_probe(self._h, int(limit)))
+
     # ---- reference-shaped entry points ------------------------------------------------
     def gdel_init(self, points, scaled=None):
         """Like gdelInit: both arrays (n,3 float64, C-contiguous) are overwritten
@@ -363,6 +371,16 @@ def _adopt(lib, ptr, nbytes, dtype, count):
     buf = (ctypes.c_char * max(nbytes, 1)).from_address(ptr)
     weakref.finalize(buf, lib.g4d_free, ctypes.c_void_p(ptr))
     return np.frombuffer(buf, dtype)[:count]
+
+
+def make_points(n, grid, dist, seed):
+    """The reference command line's points for -n -g -d -s (g4d_make_points):
+    (n, 3) float64 holding float values in grid units [1, grid-2]."""
+    out = np.empty((int(n), 3), np.float64)
+    st = load().g4d_make_points(int(n), int(dist), int(grid), int(seed), _ptr(out))
+    if st != G4D_OK:
+        raise G4DError(st, "g4d_make_points(n=%d, dist=%d, grid=%d)" % (n, dist, grid))
+    return out
 
 
 def tets_as_array(tets):

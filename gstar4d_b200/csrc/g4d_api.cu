@@ -26,14 +26,29 @@ using namespace g4d;
 
 namespace {
 
+// Allocation-failure injection for tests: with G4D_FAIL_ALLOC_AFTER=k in the
+// environment when a context is created, its workspace allocations after the
+// first k fail as if the device were out of memory (G4D_ERR_NOMEM).
+struct AllocBudget {
+    long long left = -1;  // allocations still allowed; -1: no limit
+    bool take() {
+        if (left < 0) return true;
+        if (left == 0) return false;
+        --left;
+        return true;
+    }
+};
+
 struct Buf {
     void* p = nullptr;
     size_t cap = 0;
+    AllocBudget* budget = nullptr;
     cudaError_t ensure(size_t bytes) {
         if (bytes <= cap && p) return cudaSuccess;
         if (p) cudaFree(p);
         p = nullptr;
         cap = 0;
+        if (budget && !budget->take()) return cudaErrorMemoryAllocation;
         size_t want = bytes + bytes / 8 + 256;
         cudaError_t e = cudaMalloc(&p, want);
         if (e != cudaSuccess) { p = nullptr; return e; }
@@ -68,6 +83,7 @@ struct g4d_ctx {
     cudaStream_t side = nullptr;         // proofs beside emission
     cudaEvent_t fork = nullptr, join = nullptr;
     Buf b[B_NUM];
+    AllocBudget budget;
     std::string err;
     // results of the last compute
     int n = 0;
@@ -397,7 +413,7 @@ g4d_status run_splay(g4d_ctx* ctx, Dev& D) {
     CK(cudaMemsetAsync(&dctr->emit_next, 0, 2 * sizeof(int), ctx->stream));  // emit_next, drown_next
     CK(cudaMemsetAsync(&dctr->ovf_next, 0, sizeof(int), ctx->stream));
     int loops = 0;
-    const int max_loops = 4000;
+    const int max_loops = ctx->cfg.max_splay_loops > 0 ? ctx->cfg.max_splay_loops : 4000;
     for (;; ++loops) {
         if (loops >= max_loops) return fail(ctx, G4D_ERR_TIMEOUT, "splaying did not converge in %d loops", max_loops);
         // emission phase; it only adds (deduplicated) inbox requests, so when the
@@ -620,6 +636,12 @@ g4d_status run_compute(g4d_ctx* ctx, bool map_to_input) {
         bool again = false;
         st = worksets_fit(ctx, D, attempt, &again);
         if (st) return st;
+        if (ctx->cfg.proposal && ctx->has_model) {  // the stream is idle after worksets_fit
+            MlpAux h{};
+            CK(cudaMemcpy(&h, ctx->b[B_MLP_AUX].p, sizeof(h), cudaMemcpyDeviceToHost));
+            if (h.err)
+                return fail(ctx, G4D_ERR_TIMEOUT, "tensor-core inference kernel timed out waiting (0x%x)", h.err);
+        }
         if (!again) break;
     }
     st = run_splay(ctx, D);
@@ -1150,6 +1172,10 @@ g4d_status g4d_create(g4d_ctx** out, const g4d_config* cfg) {
         return G4D_ERR_CUDA;
     }
     for (auto& e : ctx->ev) cudaEventCreate(&e);
+    if (const char* f = std::getenv("G4D_FAIL_ALLOC_AFTER")) {
+        ctx->budget.left = std::atoll(f);
+        for (auto& b : ctx->b) b.budget = &ctx->budget;
+    }
     *out = ctx;
     return G4D_OK;
 }
@@ -1495,8 +1521,13 @@ g4d_status g4d_voronoi(g4d_ctx* ctx, const double* xyz, int n, int grid, uint32_
     launch_pba_y(L, grid, ctx->b[B_GA].as<uint32_t>(), ctx->b[B_GB].as<uint32_t>());
     launch_pba_x(L, grid, ctx->b[B_GB].as<uint32_t>(), ctx->b[B_GA].as<uint32_t>());
     CK(cudaMemcpyAsync(sites, ctx->b[B_GA].p, sizeof(uint32_t) * G3, cudaMemcpyDeviceToHost, ctx->stream));
+    unsigned herr = 0;
+    CK(cudaMemcpyAsync(&herr, &ctx->b[B_CTR].as<Counters>()->err, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                       ctx->stream));
     CK_SYNC(ctx->stream);
-    return G4D_OK;
+    // coordinates the scaling could not place in [1, G-2] (NaN, infinite, or
+    // every coordinate equal) were clamped on the device: report them
+    return check_err(ctx, herr);
 }
 
 // ---- learned star proposal ------------------------------------------------
@@ -1581,7 +1612,7 @@ g4d_status g4d_proposal_train(g4d_ctx* ctx, const double* xyz, int n, int epochs
         MlpAux h{};
         CK(cudaMemcpyAsync(&h, aux, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
         CK_SYNC(ctx->stream);
-        if (h.err) return fail(ctx, G4D_ERR_INTERNAL, "tensor-core training kernel timed out waiting (0x%x)", h.err);
+        if (h.err) return fail(ctx, G4D_ERR_TIMEOUT, "tensor-core training kernel timed out waiting (0x%x)", h.err);
         last = M ? h.loss / (float)M : 0.f;
     }
     CK(cudaMemcpyAsync(ctx->mlp.data(), ctx->b[B_MLP_P].p, sizeof(float) * MLP_NPARAMS, cudaMemcpyDeviceToHost,
@@ -1631,7 +1662,7 @@ g4d_status g4d_mlp_grad(g4d_ctx* ctx, const uint16_t* x, const float* y, int m, 
     CK(cudaMemcpyAsync(grads, ctx->b[B_DIAG_G].p, sizeof(float) * MLP_NPARAMS, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaMemcpyAsync(&h, aux, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
     CK_SYNC(ctx->stream);
-    if (h.err) return fail(ctx, G4D_ERR_INTERNAL, "tensor-core training kernel timed out waiting (0x%x)", h.err);
+    if (h.err) return fail(ctx, G4D_ERR_TIMEOUT, "tensor-core training kernel timed out waiting (0x%x)", h.err);
     if (loss) *loss = h.loss / (float)m;
     return G4D_OK;
 }
@@ -1655,7 +1686,22 @@ g4d_status g4d_mlp_infer(g4d_ctx* ctx, const uint16_t* x, int m, const float* pa
     CK(cudaMemcpyAsync(logits, ctx->b[B_DIAG_Y].p, sizeof(float) * (size_t)m, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaMemcpyAsync(&h, aux, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
     CK_SYNC(ctx->stream);
-    if (h.err) return fail(ctx, G4D_ERR_INTERNAL, "tensor-core inference kernel timed out waiting (0x%x)", h.err);
+    if (h.err) return fail(ctx, G4D_ERR_TIMEOUT, "tensor-core inference kernel timed out waiting (0x%x)", h.err);
+    return G4D_OK;
+}
+
+g4d_status g4d_mlp_wait_probe(g4d_ctx* ctx, int limit) {
+    if (!ctx || limit < 1) return G4D_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    CK(ctx->b[B_MLP_AUX].ensure(sizeof(MlpAux)));
+    MlpAux* aux = ctx->b[B_MLP_AUX].as<MlpAux>();
+    CK(cudaMemsetAsync(aux, 0, sizeof(MlpAux), ctx->stream));
+    Launch L{ctx->stream, &ctx->launches};
+    launch_mlp_wait_probe(L, limit, &aux->err);
+    MlpAux h{};
+    CK(cudaMemcpyAsync(&h, aux, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+    CK_SYNC(ctx->stream);
+    if (h.err) return fail(ctx, G4D_ERR_TIMEOUT, "tensor-core kernel wait ran out after %d polls (0x%x)", limit, h.err);
     return G4D_OK;
 }
 

@@ -285,6 +285,7 @@ void launch_mlp_infer(const Launch& L, const float* P, const uint16_t* X, int M,
 void launch_mlp_train(const Launch& L, const float* P, const uint16_t* X, const float* Y, int M, const int* tiles,
                       int ntiles, float inv_batch, float* G, float* loss, unsigned* err);
 void launch_adam(const Launch& L, float* P, float* G, float* m1, float* m2, int step, float lr);
+void launch_mlp_wait_probe(const Launch& L, int limit, unsigned* err);
 struct Ring {
     const uint32_t* grid;  // Voronoi sites of the cloud's grid
     Cols<uint32_t> cols;

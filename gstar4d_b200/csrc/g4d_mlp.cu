@@ -95,9 +95,11 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar) {
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
-// bounded wait for the phase with the given parity; false after ~1 s of polling
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-    for (int i = 0; i < (1 << 20); ++i) {
+// bounded wait for the phase with the given parity; false after `limit` polls
+// (the default is about a second)
+constexpr int MBAR_LIMIT = 1 << 20;
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int limit = MBAR_LIMIT) {
+    for (int i = 0; i < limit; ++i) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
@@ -177,8 +179,8 @@ __global__ void __launch_bounds__(128, 1) k_mlp_infer(const float* __restrict__ 
     tc_after_sync();
     const uint32_t tb = S.tmem;
     const uint32_t lane_addr = tb + ((uint32_t)(warp * 32) << 16);
-    uint32_t phase = 0;
-    bool ok = true;
+    uint32_t phase = 0, failed_phase = 0;
+    bool ok = true;  // the same in every thread of the block
     const int ntiles = (M + 127) / 128;
     for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
         const int row = tile * 128 + t;
@@ -201,7 +203,13 @@ __global__ void __launch_bounds__(128, 1) k_mlp_infer(const float* __restrict__ 
                 gemm(tb + 64u * layer, a, b, 64, layer == 0 ? 16 : 64, false);
                 umma_commit(&S.bar);
             }
-            ok = mbar_wait(&S.bar, phase);
+            // a wait that ran out in any thread stops the whole block; the
+            // MMAs it waited for are drained before the tensor memory is freed
+            ok = __syncthreads_and(mbar_wait(&S.bar, phase));
+            if (!ok) {
+                failed_phase = phase;
+                break;
+            }
             phase ^= 1u;
             tc_after_sync();
             float acc = 0.f;
@@ -221,7 +229,10 @@ __global__ void __launch_bounds__(128, 1) k_mlp_infer(const float* __restrict__ 
             tc_after_sync();
         }
     }
-    if (!ok && t == 0) atomicOr(err, MLP_ERR_TIMEOUT);
+    if (!ok && t == 0) {
+        atomicOr(err, MLP_ERR_TIMEOUT);
+        mbar_wait(&S.bar, failed_phase, 4 * MBAR_LIMIT);  // the MMAs still in flight
+    }
     tc_before_sync();
     __syncthreads();
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 256;" ::"r"(tb));
@@ -290,11 +301,18 @@ __global__ void __launch_bounds__(128, 1) k_mlp_train(const float* __restrict__ 
     tc_after_sync();
     const uint32_t tb = S.tmem;
     const uint32_t lane_addr = tb + ((uint32_t)(warp * 32) << 16);
-    uint32_t phase = 0;
-    bool ok = true, any = false;
+    uint32_t phase = 0, failed_phase = 0;
+    bool ok = true, any = false;  // ok: the same in every thread of the block
     float lsum = 0.f;
-    auto sync_mma = [&]() {  // wait for the MMAs committed last
-        ok = ok && mbar_wait(&S.bar, phase);
+    // wait for the MMAs committed last. A wait that ran out in any thread
+    // clears ok in all of them: no further MMA is issued, the rest of the tile
+    // runs on stale tensor memory and is discarded, and the MMAs of the failed
+    // phase are drained before the tensor memory is freed.
+    auto sync_mma = [&]() {
+        if (ok) {
+            ok = __syncthreads_and(mbar_wait(&S.bar, phase));
+            if (!ok) failed_phase = phase;
+        }
         phase ^= 1u;
         tc_after_sync();
     };
@@ -330,7 +348,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp_train(const float* __restrict__ 
         uint32_t mask[3][2] = {{0, 0}, {0, 0}, {0, 0}};
         float z[16];
         for (int layer = 0; layer < 2; ++layer) {
-            if (t == 0) {
+            if (t == 0 && ok) {
                 gemm(tb + (layer == 0 ? TC_Z1 : TC_Z2), smem_u32(layer == 0 ? S.x : S.a1),
                      smem_u32(layer == 0 ? S.w1 : S.w2), 64, layer == 0 ? 16 : 64, false);
                 umma_commit(&S.bar);
@@ -352,7 +370,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp_train(const float* __restrict__ 
             sync_smem();
         }
         // layer 3, the logit, the loss and dz3
-        if (t == 0) {
+        if (t == 0 && ok) {
             gemm(tb + TC_Z3, smem_u32(S.a2), smem_u32(S.w3), 64, 64, false);
             umma_commit(&S.bar);
         }
@@ -391,7 +409,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp_train(const float* __restrict__ 
         }
         sync_smem();
         // da2 = dz3 W3 -> dz2
-        if (t == 0) {
+        if (t == 0 && ok) {
             gemm(tb + TC_DA2, smem_u32(S.dz3), smem_u32(S.w3t), 64, 64, false);
             umma_commit(&S.bar);
         }
@@ -413,7 +431,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp_train(const float* __restrict__ 
         }
         sync_smem();
         // da1 = dz2 W2, and [dW3; dW2] += [dz3^T; dz2^T] [a2^T; a1^T]^T
-        if (t == 0) {
+        if (t == 0 && ok) {
             gemm(tb + TC_DA1, smem_u32(S.dz2), smem_u32(S.w2t), 64, 64, false);
             gemm(tb + TC_DW, smem_u32(S.acat), smem_u32(S.bcat), 128, 128, any);
             umma_commit(&S.bar);
@@ -435,7 +453,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp_train(const float* __restrict__ 
         }
         sync_smem();
         // dW1 += [dz1^T; 0] x
-        if (t == 0) {
+        if (t == 0 && ok) {
             gemm(tb + TC_DW1, smem_u32(S.adw1), smem_u32(S.xt), 16, 128, any);
             umma_commit(&S.bar);
         }
@@ -472,10 +490,38 @@ __global__ void __launch_bounds__(128, 1) k_mlp_train(const float* __restrict__ 
         }
         if (t == 0) atomicAdd(loss_out, S.loss);
     }
-    if (!ok && t == 0) atomicOr(err, MLP_ERR_TIMEOUT);
+    if (!ok && t == 0) {
+        atomicOr(err, MLP_ERR_TIMEOUT);
+        mbar_wait(&S.bar, failed_phase, 4 * MBAR_LIMIT);  // the MMAs still in flight
+    }
     tc_before_sync();
     __syncthreads();
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tb));
+}
+
+// The waits above end after a bounded number of polls. This kernel runs the
+// same set-up (tensor memory, an mbarrier) and then waits on a phase that
+// nothing completes, with `limit` polls: the wait runs out, the kernel records
+// MLP_ERR_TIMEOUT, frees its tensor memory and returns, and the context stays
+// usable. Tests use it to exercise the timeout path without a fault.
+__global__ void __launch_bounds__(128) k_mlp_wait_probe(int limit, unsigned* err) {
+    __shared__ uint64_t bar;
+    __shared__ uint32_t tmem;
+    const int t = threadIdx.x, warp = t >> 5;
+    if (t == 0) mbar_init(&bar);
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 32;" ::"r"(smem_u32(&tmem)));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_before_sync();
+    __syncthreads();
+    tc_after_sync();
+    const uint32_t tb = tmem;
+    const bool ok = __syncthreads_and(mbar_wait(&bar, 0, limit));  // no arrival is ever made
+    if (!ok && t == 0) atomicOr(err, MLP_ERR_TIMEOUT);             // nothing in flight to drain
+    tc_before_sync();
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 32;" ::"r"(tb));
 }
 
 // Adam step on the FP32 master parameters
@@ -514,6 +560,11 @@ void launch_mlp_train(const Launch& L, const float* P, const uint16_t* X, const 
     // one CTA per SM: 512 tensor-memory columns
     int blocks = ntiles < 148 ? ntiles : 148;
     k_mlp_train<<<blocks < 1 ? 1 : blocks, 128, sm, L.stream>>>(P, X, Y, M, tiles, ntiles, inv_batch, G, loss, err);
+    ++*L.launches;
+}
+
+void launch_mlp_wait_probe(const Launch& L, int limit, unsigned* err) {
+    k_mlp_wait_probe<<<1, 128, 0, L.stream>>>(limit, err);
     ++*L.launches;
 }
 

@@ -9,16 +9,22 @@
 // allocating.
 //
 // The array is a file-scope __device__ object: every GPU that loads this
-// library holds it (about 11 MB) until the process exits. Host code sees only a
-// stand-in for it, so the device address is looked up once per device with
-// cudaGetSymbolAddress and that address is what the kernels receive. All
-// calls share the array and it keeps the previous call's contents, so calls
-// that overlap on the GPU (different streams, or several host threads) race;
-// callers must serialize them.
+// library holds it (about 9 MB) until the process exits. Host code sees only a
+// stand-in for it, so the device address is looked up with
+// cudaGetSymbolAddress, with the device current, and that address is what the
+// kernels receive. The address belongs to one CUDA context: the lookup is
+// cached per device together with the id of the context it was made in
+// (cuCtxGetId), and made again when the current context is another one (after
+// cudaDeviceReset, or under a context the caller created with the driver API).
+// All calls share the array and it keeps the previous call's contents, so
+// calls that overlap on the GPU (different streams, or several host threads)
+// race; callers must serialize them.
 //
-// The first call on each device does the set-up (the address lookup, which may
-// also load this library's kernels onto that device); make that first call
-// outside any stream capture.
+// The first call in each context does the set-up (the address lookup, which
+// may also load this library's kernels into that context); make that first
+// call outside any stream capture.
+#include <cuda.h>
+
 #include <cstdint>
 #include <cstdio>
 #include <mutex>
@@ -30,12 +36,11 @@ namespace g4d {
 constexpr int NA_MAX_POINTS = 1 << 18;  // 262,144 points
 constexpr int NA_MAX_GRID = 128;        // 128^3 voxels
 
-// scratch layout (byte offsets, each region 256-byte aligned)
+// scratch layout (byte offsets, each region 256-byte aligned); no Morton
+// sort runs here, so the scaling writes only the voxel of each point
 constexpr size_t NA_OFF_MINMAX = 0;                                               // 2 x u64
 constexpr size_t NA_OFF_ERR = 256;                                                // u32
-constexpr size_t NA_OFF_KEYS = 512;                                               // u32[NA_MAX_POINTS]
-constexpr size_t NA_OFF_VALS = NA_OFF_KEYS + 4 * (size_t)NA_MAX_POINTS;           // int[NA_MAX_POINTS]
-constexpr size_t NA_OFF_VOX = NA_OFF_VALS + 4 * (size_t)NA_MAX_POINTS;            // u32[NA_MAX_POINTS]
+constexpr size_t NA_OFF_VOX = 512;                                                // u32[NA_MAX_POINTS]
 constexpr size_t NA_OFF_GRID = NA_OFF_VOX + 4 * (size_t)NA_MAX_POINTS;            // u32[NA_MAX_GRID^3]
 constexpr size_t NA_BYTES = NA_OFF_GRID + 4 * (size_t)NA_MAX_GRID * NA_MAX_GRID * NA_MAX_GRID;
 
@@ -84,8 +89,55 @@ __global__ void k_na_zflood(int G, uint32_t* __restrict__ g, uint32_t* __restric
     }
 }
 
+// Address of the scratch array, looked up once per (device, context).
+struct NaAddr {
+    unsigned long long ctx_id;  // cuCtxGetId of the context the lookup was made in (0: none yet)
+    void* addr;
+};
 static std::mutex g_na_mutex;
-static void* g_na_addr[64];
+static NaAddr g_na_addr[64];
+
+// Id of the calling thread's current context (0 when there is none yet).
+// The driver entry points come through the runtime, so the library needs no
+// link against libcuda.
+static unsigned long long na_current_ctx_id() {
+    typedef CUresult (*GetCurrent)(CUcontext*);
+    typedef CUresult (*GetId)(CUcontext, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    if (!get_current || !get_id) {
+        void* a = nullptr;
+        void* b = nullptr;
+        cudaDriverEntryPointQueryResult qa, qb;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault, &qa) != cudaSuccess ||
+            cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault, &qb) != cudaSuccess ||
+            qa != cudaDriverEntryPointSuccess || qb != cudaDriverEntryPointSuccess || !a || !b)
+            return 0;
+        get_current = reinterpret_cast<GetCurrent>(a);
+        get_id = reinterpret_cast<GetId>(b);
+    }
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    if (get_current(&c) != CUDA_SUCCESS || !c || get_id(c, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
+
+// Device address of the scratch array in the current context, or null.
+static void* na_scratch_address(int dev) {
+    std::lock_guard<std::mutex> lk(g_na_mutex);
+    NaAddr& e = g_na_addr[dev];
+    const unsigned long long id = na_current_ctx_id();
+    if (e.addr && id != 0 && e.ctx_id == id) return e.addr;
+    void* p = nullptr;
+    // makes the device's primary context current when none is yet
+    if (cudaGetSymbolAddress(&p, g_na_scratch) != cudaSuccess || !p) {
+        (void)cudaGetLastError();
+        return nullptr;
+    }
+    e.addr = p;
+    e.ctx_id = na_current_ctx_id();  // 0 (unknown) forces a new lookup next time
+    return p;
+}
 
 }  // namespace g4d
 
@@ -103,22 +155,12 @@ extern "C" g4d_status g4d_voronoi_noalloc(const double* d_xyz, int n, int grid, 
     }
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return G4D_ERR_NODEVICE;
-    void* base = nullptr;
-    {
-        // first call on this device: look up the array's device address
-        std::lock_guard<std::mutex> lk(g_na_mutex);
-        if (!g_na_addr[dev]) {
-            void* p = nullptr;
-            if (cudaGetSymbolAddress(&p, g_na_scratch) != cudaSuccess || !p) return G4D_ERR_CUDA;
-            g_na_addr[dev] = p;
-        }
-        base = g_na_addr[dev];
-    }
+    // first call in this context: look up the array's device address
+    void* base = na_scratch_address(dev);
+    if (!base) return G4D_ERR_CUDA;
     unsigned char* s = static_cast<unsigned char*>(base);
     unsigned long long* mm = reinterpret_cast<unsigned long long*>(s + NA_OFF_MINMAX);
     unsigned* err = reinterpret_cast<unsigned*>(s + NA_OFF_ERR);
-    uint32_t* keys = reinterpret_cast<uint32_t*>(s + NA_OFF_KEYS);
-    int* vals = reinterpret_cast<int*>(s + NA_OFF_VALS);
     uint32_t* vox = reinterpret_cast<uint32_t*>(s + NA_OFF_VOX);
     uint32_t* tmp = reinterpret_cast<uint32_t*>(s + NA_OFF_GRID);
     const cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -129,7 +171,7 @@ extern "C" g4d_status g4d_voronoi_noalloc(const double* d_xyz, int n, int grid, 
         cudaMemsetAsync(err, 0, sizeof(unsigned), st) != cudaSuccess)
         return G4D_ERR_CUDA;
     launch_minmax(L, d_xyz, n, mm);
-    launch_scale_morton(L, d_xyz, nullptr, n, grid, mm, keys, vals, vox, err);
+    launch_scale_morton(L, d_xyz, nullptr, n, grid, mm, nullptr, nullptr, vox, err);
     const size_t G3 = (size_t)grid * grid * grid;
     k_na_fill<<<148 * 4, 256, 0, st>>>(d_sites, G3, MARKER);
     k_na_seed<<<(n + 255) / 256, 256, 0, st>>>(vox, n, grid, d_sites);

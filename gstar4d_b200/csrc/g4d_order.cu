@@ -76,8 +76,9 @@ __global__ void k_scale_morton(const double* __restrict__ xyz, const double* __r
             }
             q[c] = (uint32_t)v;
         }
-        keys[i] = spread10(q[0]) | (spread10(q[1]) << 1) | (spread10(q[2]) << 2);
-        vals[i] = i;
+        // keys and vals feed the Morton sort; callers without one pass null
+        if (keys) keys[i] = spread10(q[0]) | (spread10(q[1]) << 1) | (spread10(q[2]) << 2);
+        if (vals) vals[i] = i;
         vox_in[i] = enc_vox(q[0], q[1], q[2]);
     }
 }

@@ -67,6 +67,8 @@ typedef struct {
     int device;          /* CUDA device ordinal */
     int index_space;     /* 0: output indices are input indices; 1: Morton-sorted indices */
     int proposal;        /* 0: plain PBA stars; 1: learned star proposal (needs a model) */
+    int max_splay_loops; /* cap on splaying loops before G4D_ERR_TIMEOUT; 0 = 4000. The
+                            reference loops until the stars agree (GDelHost.cu:1393-1446) */
 } g4d_config;
 
 /* == Tetrahedron of Common/Geometry.h:147-150 */
@@ -196,12 +198,18 @@ G4D_API g4d_status g4d_voronoi(g4d_ctx* ctx, const double* xyz, int n, int grid,
  * values, layout as g4d_voronoi) are DEVICE pointers owned by the caller;
  * stream is a cudaStream_t (NULL: the legacy default stream). The work is
  * enqueued on that stream and the call returns without synchronizing.
- * Scratch is one fixed device array in the library (about 11.5 MB per device),
+ * Scratch is one fixed device array in the library (about 9.4 MB per device),
  * so n is at most 262144 and grid at most 128; larger sizes return
  * G4D_ERR_CAPACITY (with a message on stderr) and enqueue nothing. Every call
  * shares that array: calls that overlap on the GPU (other streams or threads)
- * race and must be serialized by the caller. The first call on each device
- * looks up the array's address; make it outside any stream capture. */
+ * race and must be serialized by the caller. The first call in each CUDA
+ * context looks up the array's address (cached with the context's id, so a
+ * cudaDeviceReset or another current context makes the next call look it up
+ * again); make that first call outside any stream capture. The call does not
+ * synchronize, so errors the device finds in the inputs (NaN or infinite
+ * coordinates, all coordinates equal) are not reported: such points are
+ * clamped into the grid and the result is meaningless. g4d_voronoi reports
+ * them as G4D_ERR_ARG. */
 G4D_API g4d_status g4d_voronoi_noalloc(const double* d_xyz, int n, int grid, uint32_t* d_sites, void* stream);
 
 /* Learned star proposal (no counterpart in the reference). A BF16 MLP scores
@@ -224,6 +232,21 @@ G4D_API g4d_status g4d_proposal_weights(g4d_ctx* ctx, float* w, int count, int s
 G4D_API g4d_status g4d_mlp_grad(g4d_ctx* ctx, const uint16_t* x, const float* y, int m, const float* params,
                                 float* grads, float* loss);
 G4D_API g4d_status g4d_mlp_infer(g4d_ctx* ctx, const uint16_t* x, int m, const float* params, float* logits);
+/* Diagnostic of the bounded waits in the tensor-core kernels: one block sets
+ * up tensor memory and an mbarrier like the MLP kernels, then waits with
+ * `limit` polls on a phase that nothing completes. The wait runs out, the
+ * kernel frees its tensor memory and returns: G4D_ERR_TIMEOUT, and the
+ * context stays usable (the path a real timeout of an MLP kernel takes). */
+G4D_API g4d_status g4d_mlp_wait_probe(g4d_ctx* ctx, int limit);
+
+/* The command line's point generator: Application::makePoints
+ * (Main/Application.cpp:316-473) with its KISS random numbers (DtRandom,
+ * Common/DtRandom.cpp:44-109, unsigned long = 64 bits as on Linux). Writes n
+ * distinct points (xyz: n*3) in grid units [1, grid-2] for distribution dist
+ * (0 uniform, 1 gaussian, 2 ball, 3 sphere, 4 grid) and seed: the float values
+ * the reference generates for -n n -g grid -d dist -s seed, held as doubles.
+ * Host code only; needs no device. */
+G4D_API g4d_status g4d_make_points(int n, int dist, int grid, int seed, double* xyz);
 
 /* The context's CUDA stream (a cudaStream_t), for callers that time or order
  * their own work against the library's launches. */
