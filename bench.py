@@ -1,18 +1,28 @@
-"""Benchmark: Mpts/s of bit-exact 3D Delaunay triangulation on B200.
+"""Benchmark: Mpts/s of bit-exact 3D Delaunay triangulation on one B200.
 
-Workload (one step = one full triangulation): the 1,000,000-point mixed cloud
-(half uniform in [0,1)^3, half N(0.5, 0.1^2) clipped), FP64, PBA grid 512^3.
+Workload (one step = one full triangulation): the 8,000,000-point clustered
+cloud (60% uniform in [0,1)^3, 40% from a 64-cluster Gaussian mixture with
+sigma 0.01), FP64, PBA grid 1024^3. `--workload` selects the other
+configurations (1M mixed at 512^3, 500k degenerate at 512^3, 100k uniform at
+256^3, the 4,096-cloud batch).
 
-  value  device throughput: points already in HBM, tetrahedra left in HBM
-  e2e    the public API with pinned host buffers: H2D of the points and D2H of
-         all tetrahedra inside every timed step
-  roofline  the PBA phase (HBM-bound) measured with CUDA events on the
-         library's stream: algorithmic bytes 20*G^3 per launch set (z pass
-         writes 4 B/voxel, y and x passes read and write 4 B/voxel)
-  cpu_baseline  the CPU oracle (a C restatement of the same pipeline, OpenMP over
-         all host cores) on a bounded sample of the same distribution
+  value      device throughput of the plain method: points already in HBM,
+             tetrahedra left in HBM
+  learned_proposal  the same step with the learned star proposal (trained,
+             untimed, on another seeded cloud of the same configuration)
+  e2e        the public API with pinned host buffers: H2D of the points and D2H
+             of all tetrahedra inside every timed step
+  roofline   the PBA phase (HBM-bound), CUDA events on the library's stream;
+             algorithmic bytes 20*G^3 per triangulation (z pass writes 4 B per
+             voxel, y and x passes read and write 4 B per voxel)
+  batch      (default line) the 4,096-cloud batch: clouds/s batched, end to
+             end, and one call per cloud
+  cpu_baseline  the CPU oracle (a C restatement of the same pipeline, OpenMP
+             over all host cores) on a random 1/8 subset of the same cloud at
+             half the grid width (same voxel density), median of 3 runs
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                    [--workload NAME]
 
 With N > 1 (torchrun) every rank triangulates its own cloud: replicas, weak
 scaling; the time is the max over ranks.
@@ -31,36 +41,34 @@ sys.path.insert(0, REPO)
 
 import numpy as np  # noqa: E402
 
-WORKLOAD = {"workload": "mixed-1M", "points": 1_000_000, "grid": 512,
-            "distribution": "50% U[0,1)^3 + 50% N(0.5,0.1^2) clipped, FP64", "seed": 1}
-# the other configurations, measured with --workload (parity cases, not the headline line)
+METRIC = "Mpts/s to bit-exact 3D DT on 1 B200: learned-proposal vs plain; batched clouds/s"
+DEFAULT_WORKLOAD = "clustered8m"
 WORKLOADS = {
-    "mixed1m": WORKLOAD,
+    "clustered8m": {"workload": "clustered-8M", "points": 8_000_000, "grid": 1024,
+                    "distribution": "60% U[0,1)^3 + 40% 64-cluster N(c, 0.01^2), FP64", "seed": 1},
+    "mixed1m": {"workload": "mixed-1M", "points": 1_000_000, "grid": 512,
+                "distribution": "50% U[0,1)^3 + 50% N(0.5,0.1^2) clipped, FP64", "seed": 1},
     "uniform100k": {"workload": "uniform-100k", "points": 100_000, "grid": 256,
                     "distribution": "U[0,1)^3, FP64", "seed": 1},
     "degenerate500k": {"workload": "degenerate-500k", "points": 500_000, "grid": 512,
                        "distribution": "50% sphere r=0.4, 30% 1/1024 lattice, 20% U[0,1)^3, FP64", "seed": 1},
-    "clustered8m": {"workload": "clustered-8M", "points": 8_000_000, "grid": 1024,
-                    "distribution": "60% U[0,1)^3 + 40% 64-cluster N(c, 0.01^2), FP64", "seed": 1},
-    "batch4096": {"workload": "batch-4096", "clouds": 4096, "grid": "per cloud (134 voxels/point rule)",
+    "batch4096": {"workload": "batch-4096", "clouds": 4096, "grid": "autotuned per (size bucket, distribution)",
                   "distribution": "sizes log-uniform in [64, 50000]; each uniform, N(0.5, 0.1^2) or 8-cluster "
                                   "N(c, 0.02^2), FP64", "seed": 1},
 }
-METRIC = "Mpts/s to bit-exact 3D DT on 1 B200"
-SAMPLE_POINTS, SAMPLE_GRID = 125_000, 256  # same voxel density (134 voxels/point)
+# CPU samples: a random 1/F subset of the workload's cloud at grid G / F^(1/3)
+# (the same voxel density). The main line's cpu_baseline uses CPU_SAMPLE (median
+# of 3 runs); the reference arm runs K + W steps, so each of its steps is the
+# smaller REF_SAMPLE and the whole arm ends within a few minutes.
+CPU_SAMPLE = {"clustered8m": 8, "mixed1m": 1, "degenerate500k": 1, "uniform100k": 1}
+REF_SAMPLE = {"clustered8m": 64, "mixed1m": 8, "degenerate500k": 8, "uniform100k": 1}
 
-
-def _pba_traffic(G):
-    """DRAM bytes of one PBA (z, y, x passes) from the committed ncu summary,
-    scaled from its grid to G by the voxel count; None when absent."""
-    try:
-        with open(os.path.join(REPO, "profiles", "pba_mixed100k_g512.md")) as f:
-            for line in f:
-                if line.startswith("traffic_per_launch_bytes:"):
-                    return float(line.split()[1]) * (G / 512.0) ** 3
-    except OSError:
-        pass
-    return None
+# DRAM traffic of one PBA (z, y and x passes) per voxel, from ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum of the three kernels, one
+# launch each, 512^3 grid); the capture and its command are in
+# profiles/pba_passes_mixed1m_g512.md. Scaled to a grid by its voxel count.
+PBA_TRAFFIC_PER_VOXEL = None
+PBA_TRAFFIC_SOURCE = "profiles/pba_passes_mixed1m_g512.md (ncu, 512^3)"
 
 
 def _peaks():
@@ -178,58 +186,100 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi, 200 ms"}
 
 
-def cpu_run(steps, threads):
-    """The oracle on the bounded sample; returns (Mpts/s, seconds per run)."""
-    from oracle import oracle_py
+def cpu_sample(workload, frac, seed):
+    """A random 1/frac subset of the workload's cloud and its grid (same voxel
+    density); frac is a power of 8."""
     from gstar4d_b200 import workloads
+    pts, G = workloads.config_cloud(workload, seed=seed)
+    if frac > 1:
+        rng = np.random.default_rng(12345)
+        keep = np.sort(rng.choice(len(pts), len(pts) // frac, replace=False))
+        pts = np.ascontiguousarray(pts[keep])
+        G = int(round(G / round(frac ** (1.0 / 3.0))))
+    return pts, G
+
+
+def cpu_run(pts, G, runs, threads):
+    """The oracle on a CPU sample; returns (Mpts/s of the median run, seconds)."""
+    from oracle import oracle_py
     oracle_py.build() if not os.path.exists(oracle_py.LIB_PATH) else None
-    pts = workloads.mixed(SAMPLE_POINTS, seed=WORKLOAD["seed"])
     times = []
-    for _ in range(steps):
+    for _ in range(runs):
         t0 = time.perf_counter()
-        oracle_py.triangulate(pts, SAMPLE_GRID, threads=threads)
+        oracle_py.triangulate(pts, G, threads=threads)
         times.append(time.perf_counter() - t0)
     t = statistics.median(times)
-    return len(pts) / t / 1e6, t, len(pts)
+    return len(pts) / t / 1e6, t
+
+
+def _sample_text(workload, frac, n, G, runs, what):
+    cfg = WORKLOADS[workload]
+    part = "random 1/%d subset (%d points) of the %s cloud" % (frac, n, cfg["workload"]) if frac > 1 else \
+        "the %s cloud (%d points)" % (cfg["workload"], n)
+    return "%s at grid %d^3 (same voxel density as %d^3), %s of %d run%s" % (
+        part, G, cfg["grid"], what, runs, "" if runs == 1 else "s")
 
 
 def reference_arm(args):
+    """The reference arm: the oracle (the reference pipeline restated in C,
+    OpenMP over all host cores) on the host; rank 0 only."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    wl = args.workload if args.workload in REF_SAMPLE else DEFAULT_WORKLOAD
     threads = os.cpu_count() or 1
-    for _ in range(max(0, min(args.warmup, 1))):
-        cpu_run(1, threads)
-    v, t, n = cpu_run(max(1, args.steps), threads)
+    frac = REF_SAMPLE[wl]
+    pts, G = cpu_sample(wl, frac, WORKLOADS[wl]["seed"])
+    for _ in range(args.warmup):
+        cpu_run(pts, G, 1, threads)
+    times = []
+    for _ in range(max(1, args.steps)):
+        _, t = cpu_run(pts, G, 1, threads)
+        times.append(t)
+    total = sum(times)
+    v = len(pts) * len(times) / total / 1e6
     line = {
         "impl": "reference", "metric": METRIC, "value": round(v, 4), "unit": "Mpts/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t * 1e3, 3), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": dict(WORKLOAD),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(total / len(times) * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": dict(WORKLOADS[wl]),
         "cpu_baseline": {"value": round(v, 4), "unit": "Mpts/s", "cores": threads, "kind": "port",
-                         "sample": "%d-point mixed cloud at grid %d^3 (same distribution and voxel density), "
-                                   "median of %d runs" % (n, SAMPLE_GRID, max(1, args.steps))},
+                         "sample": _sample_text(wl, frac, len(pts), G, len(times), "total time")},
         "e2e": {"value": round(v, 4), "unit": "Mpts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
     return 0
 
 
-def batch_main(args):
+def _timed(fn, ext, flush, steps):
+    """Device time of `steps` calls of fn on the library's stream (CUDA events,
+    the L2 flushed before each); returns (list of ms, last result)."""
+    import torch
+    ms, res = [], None
+    for _ in range(steps):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(ext)
+        res = fn()
+        e.record(ext)
+        e.synchronize()
+        ms.append(s.elapsed_time(e))
+    return ms, res
+
+
+def run_batch(args, local, rank, steps):
     """4,096 clouds with autotuned grid widths. value: clouds/s of the batched
     call on device-resident points (tetrahedra left on the device); e2e: the
     batched call from pinned host points into a pinned host buffer;
-    one_call_per_cloud: the same clouds through one host call each (same
-    widths, same context)."""
+    one_call_per_cloud: the same clouds through one call each (same widths,
+    same context)."""
     import torch
     import gstar4d_b200
     from gstar4d_b200 import workloads
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
     cfg = dict(WORKLOADS["batch4096"])
     clouds, pts, offs = workloads.batch_clouds(cfg["clouds"], seed=cfg["seed"] + rank)
-    tri = gstar4d_b200.Triangulator(grid_size=-1, device=local, log_verbose=int(os.environ.get("G4D_VERBOSE", "0")))
+    tri = gstar4d_b200.Triangulator(grid_size=-1, device=local)
     ext = torch.cuda.ExternalStream(tri.stream, device=local)
     d_pts = torch.from_numpy(pts).to(f"cuda:{local}")
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device=f"cuda:{local}")
@@ -237,17 +287,9 @@ def batch_main(args):
         tri.triangulate_batch_device(d_pts.data_ptr(), offs)
     sampler = ClockSampler(local)
     sampler.start()
-    ms = []
-    for _ in range(args.steps):
-        flush.fill_(1)
-        torch.cuda.synchronize()
-        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s.record(ext)
-        _, ntet, _, st = tri.triangulate_batch_device(d_pts.data_ptr(), offs)
-        e.record(ext)
-        e.synchronize()
-        ms.append(s.elapsed_time(e))
+    ms, res = _timed(lambda: tri.triangulate_batch_device(d_pts.data_ptr(), offs), ext, flush, steps)
     clocks = sampler.stop()
+    _, ntet, _, st = res
     value = len(clouds) / (statistics.mean(ms) / 1e3)
     # end to end: pinned host points in, pinned host tetrahedra out (copied
     # pass by pass while later passes compute)
@@ -255,78 +297,71 @@ def batch_main(args):
     h_out = torch.empty((int(ntet * 1.02) + 4096, 8), dtype=torch.int32).pin_memory()
     pts_np, out_np = h_pts.numpy(), h_out.numpy().view(gstar4d_b200.TET_DTYPE).reshape(-1)
     tri.triangulate_batch(pts_np, offs, out=out_np)
-    e2e_ms = []
-    for _ in range(args.steps):
-        flush.fill_(1)
-        torch.cuda.synchronize()
-        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s.record(ext)
-        tets, toffs, _ = tri.triangulate_batch(pts_np, offs, out=out_np)
-        e.record(ext)
-        e.synchronize()
-        e2e_ms.append(s.elapsed_time(e))
+    e2e_ms, _ = _timed(lambda: tri.triangulate_batch(pts_np, offs, out=out_np), ext, flush, steps)
     e2e = len(clouds) / (statistics.mean(e2e_ms) / 1e3)
-    # one call per cloud through the same context (same tuned widths): device-
-    # resident points and tetrahedra, and host points to host tetrahedra
+    # one call per cloud through the same context (same tuned widths)
     for c in range(8):
         tri.triangulate_device(d_pts[offs[c]:offs[c + 1]].data_ptr(), int(offs[c + 1] - offs[c]))
         tri.triangulate(clouds[c])
-    torch.cuda.synchronize()
-    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    s.record(ext)
-    for c in range(len(clouds)):
-        tri.triangulate_device(d_pts[offs[c]:offs[c + 1]].data_ptr(), int(offs[c + 1] - offs[c]))
-    e.record(ext)
-    e.synchronize()
-    single_dev_ms = s.elapsed_time(e)
+
+    def singles_device():
+        for c in range(len(clouds)):
+            tri.triangulate_device(d_pts[offs[c]:offs[c + 1]].data_ptr(), int(offs[c + 1] - offs[c]))
+
+    def singles_host():
+        for c in clouds:
+            tri.triangulate(c)
+
+    (single_dev_ms,), _ = _timed(singles_device, ext, flush, 1)
+    (single_ms,), _ = _timed(singles_host, ext, flush, 1)
     single_dev = len(clouds) / (single_dev_ms / 1e3)
-    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    s.record(ext)
-    for c in clouds:
-        tri.triangulate(c)
-    e.record(ext)
-    e.synchronize()
-    single_ms = s.elapsed_time(e)
     single = len(clouds) / (single_ms / 1e3)
-    if rank == 0:
-        line = {
-            "metric": "clouds/s, 4096-cloud batch to bit-exact 3D DT on 1 B200", "value": round(value, 1),
-            "unit": "clouds/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": round(statistics.mean(ms), 3), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": dict(cfg, points=int(offs[-1]), grid="autotuned per (size bucket, distribution)",
-                           l2="256 MB buffer written between timed steps; inputs 737 MB"),
-            "e2e": {"value": round(e2e, 1), "unit": "clouds/s", "h2d_bytes_per_step": int(offs[-1]) * 24,
-                    "d2h_bytes_per_step": int(ntet) * 32},
-            "one_call_per_cloud": {"value": round(single_dev, 1), "unit": "clouds/s",
-                                   "ms": round(single_dev_ms, 1),
-                                   "api": "device-resident points and tetrahedra, one call per cloud"},
-            "one_call_per_cloud_e2e": {"value": round(single, 1), "unit": "clouds/s", "ms": round(single_ms, 1),
-                                       "api": "host points in, host tetrahedra out, one call per cloud"},
-            "batched_over_one_call_per_cloud": round(value / single_dev, 2),
-            "batched_over_one_call_per_cloud_e2e": round(e2e / single, 2),
-            "splay": {"loops_max": st["loops"], "insertions": st["splay_insertions"], "tets": int(ntet),
-                      "large_stars": st["large_stars"]},
-            "stages_ms": {k: round(st[k], 3) for k in ("t_init_ms", "t_pba_ms", "t_star_ms", "t_splay_ms",
-                                                        "t_out_ms", "t_total_ms")},
-            "clocks": clocks, "gpu_launches": int(st["gpu_launches"]),
-        }
-        print(json.dumps(line))
     tri.close()
+    return {
+        "metric": "clouds/s, 4096-cloud batch to bit-exact 3D DT on 1 B200", "value": round(value, 1),
+        "unit": "clouds/s", "steps": steps, "ms_per_step": round(statistics.mean(ms), 3),
+        "config": dict(cfg, points=int(offs[-1]), l2="256 MB buffer written between timed steps; inputs 737 MB"),
+        "e2e": {"value": round(e2e, 1), "unit": "clouds/s", "h2d_bytes_per_step": int(offs[-1]) * 24,
+                "d2h_bytes_per_step": int(ntet) * 32},
+        "one_call_per_cloud": {"value": round(single_dev, 1), "unit": "clouds/s", "ms": round(single_dev_ms, 1),
+                               "api": "device-resident points and tetrahedra, one call per cloud"},
+        "one_call_per_cloud_e2e": {"value": round(single, 1), "unit": "clouds/s", "ms": round(single_ms, 1),
+                                   "api": "host points in, host tetrahedra out, one call per cloud"},
+        "batched_over_one_call_per_cloud": round(value / single_dev, 2),
+        "batched_over_one_call_per_cloud_e2e": round(e2e / single, 2),
+        "splay": {"loops_max": st["loops"], "insertions": st["splay_insertions"], "tets": int(ntet),
+                  "large_stars": st["large_stars"]},
+        "stages_ms": {k: round(st[k], 3) for k in ("t_init_ms", "t_pba_ms", "t_star_ms", "t_splay_ms",
+                                                    "t_out_ms", "t_total_ms")},
+        "clocks": clocks, "gpu_launches": int(st["gpu_launches"]) * steps,
+    }
+
+
+def batch_main(args):
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank = int(os.environ.get("RANK", "0"))
+    import torch
+    torch.cuda.set_device(local)
+    b = run_batch(args, local, rank, args.steps)
+    if rank == 0:
+        line = dict(b, n_gpus=1, warmup=args.warmup, higher_is_better=True, scaling="weak", vs_baseline=None,
+                    dtype="f64", data="synthetic")
+        print(json.dumps(line))
     return 0
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="mixed1m", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--points", type=int, default=None)
     ap.add_argument("--grid", type=int, default=None)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -347,11 +382,11 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     cfg = dict(WORKLOADS[args.workload])
+    base_points = cfg["points"]
     args.points = args.points or cfg["points"]
     args.grid = args.grid or cfg["grid"]
     cfg["points"], cfg["grid"] = args.points, args.grid
-    pts, _ = workloads.config_cloud(args.workload, scale=args.points / WORKLOADS[args.workload]["points"],
-                                    seed=cfg["seed"] + rank)
+    pts, _ = workloads.config_cloud(args.workload, scale=args.points / base_points, seed=cfg["seed"] + rank)
     n = len(pts)
     tri = gstar4d_b200.Triangulator(grid_size=args.grid, device=local)
     ext = torch.cuda.ExternalStream(tri.stream, device=local)
@@ -364,75 +399,72 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
+    def max_over_ranks(x):
+        if world > 1:
+            t = torch.tensor([x], device=f"cuda:{local}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            return float(t.item())
+        return x
+
     # ---- device throughput (value) ----
     for _ in range(args.warmup):
         tri.triangulate_device(d_pts.data_ptr(), n)
     barrier()
     sampler = ClockSampler(local)
     sampler.start()
-    step_ms, pba_ms, launches, ntets = [], [], 0, 0
-    for _ in range(args.steps):
-        flush.fill_(1)
-        torch.cuda.synchronize()
-        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s.record(ext)
-        _, ntets, st = tri.triangulate_device(d_pts.data_ptr(), n)
-        e.record(ext)
-        e.synchronize()
-        step_ms.append(s.elapsed_time(e))
-        pba_ms.append(st["t_pba_ms"])
-        launches += st["gpu_launches"]
-        last = st
+    stats = []
+
+    def step():
+        r = tri.triangulate_device(d_pts.data_ptr(), n)
+        stats.append(r[2])
+        return r
+
+    step_ms, (_, ntets, last) = _timed(step, ext, flush, args.steps)
     barrier()
     clocks = sampler.stop()
-    total_ms = sum(step_ms)
-    if world > 1:
-        t = torch.tensor([total_ms], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(sum(step_ms))
     value = world * n * args.steps / (total_ms / 1e3) / 1e6
+    pba_ms = [s["t_pba_ms"] for s in stats]
+    launches = sum(int(s["gpu_launches"]) for s in stats)
 
     # ---- learned star proposal: trained (untimed) on another seeded cloud of the
-    # same distribution with labels from the plain method, then timed like value
+    # same configuration with labels from the plain method, then timed like value
     learned = None
     if not args.no_learned:
-        train_pts, _ = workloads.config_cloud(args.workload, scale=args.points / WORKLOADS[args.workload]["points"],
+        train_pts, _ = workloads.config_cloud(args.workload, scale=args.points / base_points,
                                               seed=cfg["seed"] + 1000 + rank)
         with gstar4d_b200.Triangulator(grid_size=args.grid, device=local) as tt:
             t0 = time.perf_counter()
             loss = tt.train_proposal(train_pts, epochs=4, lr=2e-3)
             train_s = time.perf_counter() - t0
             weights = tt.proposal_weights()
+        del train_pts
         tl = gstar4d_b200.Triangulator(grid_size=args.grid, device=local, proposal=1)
         tl.proposal_weights(weights)
         extl = torch.cuda.ExternalStream(tl.stream, device=local)
         for _ in range(args.warmup):
             tl.triangulate_device(d_pts.data_ptr(), n)
         barrier()
-        lms = []
-        for _ in range(args.steps):
-            flush.fill_(1)
-            torch.cuda.synchronize()
-            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            s.record(extl)
-            _, ntl, stl = tl.triangulate_device(d_pts.data_ptr(), n)
-            e.record(extl)
-            e.synchronize()
-            lms.append(s.elapsed_time(e))
+        lstats = []
+
+        def lstep():
+            r = tl.triangulate_device(d_pts.data_ptr(), n)
+            lstats.append(r[2])
+            return r
+
+        lms, (_, ntl, stl) = _timed(lstep, extl, flush, args.steps)
         barrier()
-        lt = sum(lms)
-        if world > 1:
-            tt_ = torch.tensor([lt], device=f"cuda:{local}")
-            dist.all_reduce(tt_, op=dist.ReduceOp.MAX)
-            lt = float(tt_.item())
-        learned = {"value": round(world * n * args.steps / (lt / 1e3) / 1e6, 3), "unit": "Mpts/s",
-                   "ms_per_step": round(lt / args.steps, 3), "tets": ntl,
+        lt = max_over_ranks(sum(lms))
+        launches += sum(int(s["gpu_launches"]) for s in lstats)
+        lv = world * n * args.steps / (lt / 1e3) / 1e6
+        learned = {"value": round(lv, 3), "unit": "Mpts/s", "over_plain": round(lv / value, 3),
+                   "ms_per_step": round(lt / args.steps, 3), "tets": ntl, "same_tets_as_plain": ntl == ntets,
                    "star_insertions_per_point": round(stl["star_insertions"] / n, 3),
                    "splay_insertions_per_point": round(stl["splay_insertions"] / n, 3),
                    "proposed_per_point": round(stl["proposed"] / n, 3), "loops": stl["loops"],
                    "stages_ms": {k: round(stl[k], 3) for k in ("t_pba_ms", "t_star_ms", "t_splay_ms", "t_out_ms")},
-                   "training": {"cloud": "same distribution, seed + 1000", "epochs": 4, "final_loss": round(loss, 4),
-                                "seconds": round(train_s, 2)}}
+                   "training": {"cloud": "same configuration, seed + 1000", "epochs": 4,
+                                "final_loss": round(loss, 4), "seconds": round(train_s, 2)}}
         tl.close()
 
     # ---- end to end through the public API with pinned host buffers ----
@@ -444,22 +476,18 @@ def main():
     for _ in range(max(1, min(args.warmup, 2))):
         tri.triangulate(pts_np, out=out_np)
     barrier()
-    e2e_ms = []
-    for _ in range(args.steps):
-        flush.fill_(1)
-        torch.cuda.synchronize()
-        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s.record(ext)
-        tets, _, _ = tri.triangulate(pts_np, out=out_np)
-        e.record(ext)
-        e.synchronize()
-        e2e_ms.append(s.elapsed_time(e))
-    e2e_total = sum(e2e_ms)
-    if world > 1:
-        t = torch.tensor([e2e_total], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_total = float(t.item())
+    e2e_ms, (tets, _, _) = _timed(lambda: tri.triangulate(pts_np, out=out_np), ext, flush, args.steps)
+    e2e_total = max_over_ranks(sum(e2e_ms))
     e2e = world * n * args.steps / (e2e_total / 1e3) / 1e6
+    ntet_e2e = len(tets)
+    tri.close()
+    del d_pts, h_out, out_np, tets
+    torch.cuda.empty_cache()
+
+    # ---- the 4,096-cloud batch (extra key of the default line, N = 1) ----
+    batch = None
+    if world == 1 and not args.no_batch and args.workload == DEFAULT_WORKLOAD:
+        batch = run_batch(args, local, rank, min(args.steps, 5))
 
     if rank == 0:
         peak, peak_kind = _peaks()
@@ -467,16 +495,18 @@ def main():
         alg_bytes = 20.0 * G ** 3
         pba_avg = statistics.mean(pba_ms)
         achieved = alg_bytes / (pba_avg / 1e3) / 1e9
+        traffic = PBA_TRAFFIC_PER_VOXEL * G ** 3 if PBA_TRAFFIC_PER_VOXEL else None
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "Mpts/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": dict(cfg, l2="256 MB buffer written between timed steps", parallelism="replicas"),
+            "config": dict(cfg, method="plain PBA stars (learned proposal in learned_proposal)",
+                           l2="256 MB buffer written between timed steps", parallelism="replicas"),
             "e2e": {"value": round(e2e, 3), "unit": "Mpts/s", "h2d_bytes_per_step": int(n * 24),
-                    "d2h_bytes_per_step": int(len(tets) * 32)},
-            "roofline": {"kernel": "pba (z,y,x passes)", "bound": "hbm", "achieved": round(achieved, 1),
+                    "d2h_bytes_per_step": int(ntet_e2e * 32)},
+            "roofline": {"kernel": "pba (z, y, x passes)", "bound": "hbm", "achieved": round(achieved, 1),
                          "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                         "traffic": _pba_traffic(G), "traffic_source": "profiles/pba_mixed100k_g512.md (ncu)",
+                         "traffic": traffic, "traffic_source": PBA_TRAFFIC_SOURCE if traffic else None,
                          "algorithmic_bytes": alg_bytes, "avg_ms": round(pba_avg, 4)},
             "stages_ms": {k: round(last[k], 3) for k in ("t_init_ms", "t_pba_ms", "t_star_ms", "t_splay_ms",
                                                           "t_out_ms", "t_total_ms")},
@@ -485,17 +515,18 @@ def main():
                       "proofs": last["proofs"], "exact_predicates": last["exact_predicates"],
                       "large_stars": last["large_stars"], "tets": ntets},
             "learned_proposal": learned,
+            "batch": batch,
             "clocks": clocks,
             "gpu_launches": int(launches),
         }
-        if not args.no_cpu and world == 1:  # the CPU baseline is an N=1 figure
+        if not args.no_cpu and world == 1 and args.workload in CPU_SAMPLE:  # an N=1 figure
             threads = os.cpu_count() or 1
-            v, t, ns = cpu_run(1, threads)
+            frac = CPU_SAMPLE[args.workload]
+            cp, cG = cpu_sample(args.workload, frac, cfg["seed"])
+            v, t = cpu_run(cp, cG, 3, threads)
             line["cpu_baseline"] = {"value": round(v, 4), "unit": "Mpts/s", "cores": threads, "kind": "port",
-                                    "sample": "%d-point mixed cloud at grid %d^3 (same distribution and voxel "
-                                              "density), one run" % (ns, SAMPLE_GRID)}
+                                    "sample": _sample_text(args.workload, frac, len(cp), cG, 3, "median")}
         print(json.dumps(line))
-    tri.close()
     if world > 1:
         dist.destroy_process_group()
     return 0
