@@ -26,9 +26,11 @@ points are the reference's own: its makePoints and KISS generator (DtRandom,
 -f, -predThreadNum and -predBlockNum are accepted and have no effect (no
 per-loop facet bound, no fixed exact-predicate thread pool). -proposal loads
 learned star-proposal weights (float32[9473], see Triangulator.train_proposal).
--float rounds the points to float32 first, like the reference's default
-RealType = float build (Common/Geometry.h:53-57, file input parsed as float at
-Application.cpp:501-511); the triangulation is then that of the float values.
+-float follows the reference's default RealType = float build
+(Common/Geometry.h:53-57): file input is scaled in float arithmetic, so the
+scaled points are the float build's (generated points are float values in
+both builds); the predicates are exact in both builds, so the triangulation is
+that build's.
 """
 import sys
 import time
@@ -109,12 +111,19 @@ def read_point_file(path):
     return np.ascontiguousarray(pts[keep]), mn, mx, len(pts) - len(keep)
 
 
-def scale_points(points, grid, mn, mx):
+def scale_points(points, grid, mn, mx, as_float=False):
     """_scalePoint (Application.cpp:589-603): v -> (G - 3) (v - min) / (max -
     min) + 1 with the float bounds (their difference taken in float), the rest
-    in double; duplicates the scaling creates are dropped."""
-    rng = np.float64(np.float32(mx) - np.float32(mn))
-    p = (float(grid) - 3.0) * (np.asarray(points, np.float64) - np.float64(mn)) / rng + 1.0
+    in RealType: double (the REAL_TYPE_DOUBLE build), or float with as_float
+    (the default float build, Common/Geometry.h:53-57, where every step rounds
+    to float). Duplicates the scaling creates are dropped."""
+    f32 = np.float32
+    rng = f32(mx) - f32(mn)
+    if as_float:
+        t = np.asarray(points, np.float64).astype(f32) - f32(mn)
+        p = ((f32(grid) - f32(3.0)) * t / rng + f32(1.0)).astype(np.float64)
+    else:
+        p = (float(grid) - 3.0) * (np.asarray(points, np.float64) - np.float64(mn)) / np.float64(rng) + 1.0
     _, first = np.unique(p, axis=0, return_index=True)
     return np.ascontiguousarray(p[np.sort(first)])
 
@@ -215,16 +224,15 @@ def main(argv=None):
             raw, mn, mx, dups = read_point_file(o["in_file"])
             if dups:
                 print("%d duplicate points in input file!" % dups)
-            pts = scale_points(raw, o["grid"], mn, mx)
+            pts = scale_points(raw, o["grid"], mn, mx, as_float=o["float"])
             if o["stats"]:
                 print("Min: %g Max: %g Min-Scaled: %g Max-Scaled: %g" % (
                     mn, mx, 1.0, (o["grid"] - 3.0) + 1.0))
             if o["out_file"]:
                 write_asc("Input-Scaled-Points.asc", pts)
         else:
+            # float values already: the same points in both of the reference's builds
             pts = make_points(o["n"], o["grid"], o["dist"], seed)
-            if o["float"]:
-                pts = as_float_values(pts)
             if o["out_file"]:
                 write_asc("Input-Points.asc", pts)
         n_used = len(pts)

@@ -12,16 +12,21 @@
  * at build time (sed, into oracle/_ref/, never committed) and compiles them
  * against the small stand-ins below for the class and types they use;
  * Config.h, DtRandom.h and DtRandom.cpp are compiled as they are. Point3 is
- * the REAL_TYPE_DOUBLE layout (Common/Geometry.h:53-69).
+ * the REAL_TYPE_DOUBLE layout (Common/Geometry.h:53-69), or with
+ * REF_REAL_FLOAT defined the default float build's (RealType = float), whose
+ * file scaling runs in float arithmetic.
  */
 #include "Config.h"
 #include "DtRandom.h"
 
 #include <algorithm>
 #include <cassert>
-#include <cstring>
 
+#ifdef REF_REAL_FLOAT
+typedef float RealType;
+#else
 typedef double RealType;
+#endif
 
 struct Point3 {
     RealType _p[3];
@@ -96,7 +101,7 @@ void ref_morton_keys(const double* pts, int n, int* keys) {
     GetMortonNumber f;
     for (int i = 0; i < n; ++i) {
         Point3 p;
-        std::memcpy(p._p, pts + 3 * (size_t)i, sizeof(p._p));
+        for (int k = 0; k < 3; ++k) p._p[k] = (RealType)pts[3 * (size_t)i + k];
         keys[i] = f(p);
     }
 }

@@ -63,7 +63,7 @@ def test_float_flag_rounds_points_to_float32(tmp_path):
     p = cli.read_points(str(f), as_float=True)
     assert p.dtype == np.float64 and len(p) == 2
     assert np.array_equal(p[0], np.array([0.1, 0.2, 0.3], np.float32).astype(np.float64))
-    g = cli.as_float_values(cli.make_points(2000, 64, 0, seed=1))
+    g = cli.as_float_values(cli.make_points(2000, 64, 0, seed=1) * 1.1)
     assert np.array_equal(g, g.astype(np.float32).astype(np.float64))
 
 

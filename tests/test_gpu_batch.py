@@ -130,3 +130,29 @@ def test_batch_into_pinned_buffer_over_many_passes(oracle, monkeypatch):
         with pytest.raises(gstar4d_b200.G4DError) as e:
             t.triangulate_batch(pts, offs, out=short)
         assert e.value.status == 1
+
+
+def test_batch_of_64_clouds_from_the_4096_generator_matches_oracle(oracle):
+    """The first 64 clouds of the 4,096-cloud benchmark generator (sizes
+    log-uniform up to 50,000; uniform, Gaussian and 8-cluster clouds), batched
+    at the reference's density rule and with autotuned widths, every cloud
+    compared with the oracle. The clouds are in general position, so the
+    triangulation does not depend on the grid width the tuner picks."""
+    import gstar4d_b200
+    sizes = workloads.batch_sizes(4096, seed=1)[:64]
+    kinds = np.random.default_rng(1 + 7).integers(0, 3, size=4096)[:64]
+    clouds = [workloads.batch_cloud(int(n), int(k), 1 * 100003 + i) for i, (n, k) in enumerate(zip(sizes, kinds))]
+    assert max(len(c) for c in clouds) > 20000
+    offs = np.zeros(len(clouds) + 1, np.int64)
+    offs[1:] = np.cumsum([len(c) for c in clouds])
+    pts = np.concatenate(clouds)
+    refs = [oracle.canonical(oracle.triangulate(c, auto_grid(len(c)))[0]) for c in clouds]
+    for grid in (0, -1):
+        with gstar4d_b200.Triangulator(grid_size=grid) as t:
+            if grid < 0:
+                t.triangulate_batch(pts, offs)  # the first call tunes the widths
+            tets, toffs, _ = t.triangulate_batch(pts, offs)
+        for c in range(len(clouds)):
+            got = _canon(oracle, tets[toffs[c]:toffs[c + 1]])
+            assert np.array_equal(got[0], refs[c][0]), "grid %d, cloud %d: tetrahedra differ" % (grid, c)
+            assert np.array_equal(got[1], refs[c][1]), "grid %d, cloud %d: adjacency differs" % (grid, c)

@@ -117,3 +117,50 @@ def test_read_points_equals_reference(ref, tmp_path):
         got = cli.scale_points(raw, grid, mn, mx)
         assert dup == 10 and m == len(got)
         assert got.tobytes() == np.ascontiguousarray(want[:m]).tobytes()
+
+
+REF_APP_F32 = os.path.join(REPO, "oracle", "_ref", "libref_app_f32.so")
+
+
+@pytest.fixture(scope="module")
+def ref32():
+    if not os.path.exists(REF_APP_F32):
+        pytest.skip("float build of the reference host code not built here")
+    R = ctypes.CDLL(REF_APP_F32)
+    vp = ctypes.c_void_p
+    R.ref_make_points.argtypes = [ctypes.c_int] * 4 + [vp]
+    R.ref_read_points.argtypes = [ctypes.c_char_p, ctypes.c_int, vp, ctypes.c_int]
+    R.ref_scale_value.argtypes = [ctypes.c_double, ctypes.c_float, ctypes.c_float, ctypes.c_double]
+    R.ref_scale_value.restype = ctypes.c_double
+    return R
+
+
+def test_float_build_file_input_equals_reference(ref32, tmp_path):
+    """The default float build (RealType = float) scales file input in float
+    arithmetic; the command line's -float mode must give its scaled points."""
+    from gstar4d_b200 import __main__ as cli
+    rng = np.random.default_rng(11)
+    pts = np.concatenate([rng.normal(-2.0, 40.0, (3000, 3)), rng.random((1000, 3))])
+    f = tmp_path / "pts.txt"
+    with open(f, "w") as fh:
+        for p in pts:
+            fh.write("%.8g %.8g %.8g\n" % tuple(p))
+    for grid in (64, 256, 1024):
+        want = np.empty((len(pts), 3))
+        m = ref32.ref_read_points(str(f).encode(), grid, _p(want), len(pts))
+        raw, mn, mx, _ = cli.read_point_file(str(f))
+        got = cli.scale_points(raw, grid, mn, mx, as_float=True)
+        assert m == len(got)
+        assert got.tobytes() == np.ascontiguousarray(want[:m]).tobytes()
+        # and the double build differs in general (the scaling rounds differently)
+        dbl = cli.scale_points(raw, grid, mn, mx)
+        assert not np.array_equal(dbl, got)
+
+
+def test_float_build_generates_the_same_points(ref, ref32):
+    for dist in range(5):
+        a = np.empty((3000, 3))
+        b = np.empty((3000, 3))
+        ref.ref_make_points(3000, dist, 128, 2, _p(a))
+        ref32.ref_make_points(3000, dist, 128, 2, _p(b))
+        assert a.tobytes() == b.tobytes()
