@@ -175,27 +175,27 @@ def write_ply(path, points, tets):
         np.savetxt(f, np.concatenate([np.full((len(faces), 1), 3), faces], axis=1), fmt="%d")
 
 
-def check_adjacency(tets):
-    """Host check of the output: every neighbour link is reciprocated across the
-    same face. Returns the number of broken links."""
-    v = tets["v"].astype(np.int64)
-    opp = tets["opp"].astype(np.int64)
-    bad = 0
-    faces = {}
-    for t in range(len(v)):
-        for i in range(4):
-            key = tuple(sorted(np.delete(v[t], i)))
-            faces.setdefault(key, []).append((t, i))
-    for t in range(len(v)):
-        for i in range(4):
-            n = opp[t, i]
-            key = tuple(sorted(np.delete(v[t], i)))
-            mates = [u for u, _ in faces[key] if u != t]
-            if n < 0:
-                bad += len(mates) != 0
-            else:
-                bad += mates != [n]
-    return bad
+def print_check(rep):
+    """The device validator's report in TetraMesh::check's words
+    (Common/Geometry.cu:200-393); returns True when the mesh passed."""
+    print("Euler Characteristic:")
+    print("V: %d E: %d F: %d T: %d Euler: %d" % (rep["vertices"], rep["edges"], rep["triangles"], rep["tets"],
+                                                 rep["euler"]))
+    if rep["euler"] != 1:
+        print("Euler check failed!")
+    if rep["orient_fail"]:
+        print("Orientation check failed!!!")
+        print("Tetra failures: %d" % rep["orient_fail"])
+    else:
+        print("Tetra orientation is correct!")
+    if rep["insphere_fail"]:
+        print("In-sphere check failed!!!")
+        print("Tetra failures: %d" % rep["insphere_fail"])
+    else:
+        print("Tetra in-sphere is correct!")
+    if rep["adjacency_fail"]:
+        print("Adjacency check failed: %d links" % rep["adjacency_fail"])
+    return rep["euler"] == 1 and not (rep["orient_fail"] or rep["insphere_fail"] or rep["adjacency_fail"])
 
 
 def main(argv=None):
@@ -245,7 +245,8 @@ def main(argv=None):
             init_ms = (time.perf_counter() - t0) * 1e3
             times = t.gdel_compute()
             tot_ms = (time.perf_counter() - t0) * 1e3
-            tets = t.get_tetra_from_gpu() if (o["check"] or o["out_file"]) else None
+            tets = t.get_tetra_from_gpu() if o["out_file"] else None
+            rep = t.check_mesh() if o["check"] else None
             st = t.stats()
             t.gdel_deinit()
         print("")
@@ -265,11 +266,8 @@ def main(argv=None):
         if o["stats"] or o["verbose"]:
             print("Star insertions: %d  Splay insertions: %d  Loops: %d  Tetra: %d  Exact predicates: %d" % (
                 st["star_insertions"], st["splay_insertions"], st["loops"], st["tets"], st["exact_predicates"]))
-        if o["check"]:
-            bad = check_adjacency(tets)
-            print("Check: stars consistent on the device; %s" % (
-                "adjacency OK" if bad == 0 else "%d adjacency links broken" % bad))
-            if bad:
+        if o["check"]:  # star consistency ran on the device during splaying; then the mesh validator
+            if not print_check(rep):
                 return 2
         if o["out_file"]:
             write_ply(o["out_file"], work, tets)  # the tetrahedra index the Morton-sorted points

@@ -41,6 +41,14 @@ class Config(ctypes.Structure):
                 ("proposal", ctypes.c_int), ("max_splay_loops", ctypes.c_int)]
 
 
+class CheckReport(ctypes.Structure):
+    _fields_ = [(f, ctypes.c_longlong) for f in ("vertices", "edges", "triangles", "tets", "euler", "orient_fail",
+                                                 "insphere_fail", "adjacency_fail")]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 class Stats(ctypes.Structure):
     _fields_ = [("t_init_ms", ctypes.c_double), ("t_pba_ms", ctypes.c_double), ("t_star_ms", ctypes.c_double),
                 ("t_splay_ms", ctypes.c_double), ("t_out_ms", ctypes.c_double), ("t_total_ms", ctypes.c_double),
@@ -64,7 +72,7 @@ EXPORTS = ["g4d_default_config", "g4d_create", "g4d_destroy", "g4d_last_error", 
            "g4d_gdel_compute", "g4d_get_tetra", "g4d_gdel_deinit", "g4d_get_stats", "g4d_triangulate_batch",
            "g4d_triangulate_batch_to", "g4d_triangulate_batch_device", "g4d_stream",
            "g4d_eval_predicates", "g4d_voronoi", "g4d_voronoi_noalloc", "g4d_proposal_train",
-           "g4d_proposal_weights", "g4d_mlp_grad", "g4d_mlp_infer", "g4d_mlp_wait_probe", "g4d_make_points", "g4d_free"]
+           "g4d_proposal_weights", "g4d_mlp_grad", "g4d_mlp_infer", "g4d_mlp_wait_probe", "g4d_make_points", "g4d_check_mesh", "g4d_check_tets", "g4d_free"]
 
 MLP_PARAMS = 9473
 
@@ -110,6 +118,8 @@ def load():
     L.g4d_mlp_infer.argtypes = [vp, vp, ip, vp, vp]
     L.g4d_mlp_wait_probe.argtypes = [vp, ip]
     L.g4d_make_points.argtypes = [ip, ip, ip, ip, vp]
+    L.g4d_check_mesh.argtypes = [vp, ctypes.POINTER(CheckReport)]
+    L.g4d_check_tets.argtypes = [vp, vp, ip, vp, ip, ctypes.POINTER(CheckReport)]
     L.g4d_stream.argtypes = [vp]
     L.g4d_stream.restype = vp
     L.g4d_free.argtypes = [vp]
@@ -275,6 +285,25 @@ class Triangulator:
         out = np.empty(len(x), np.float32)
         self._check(self._lib.g4d_mlp_infer(self._h, _ptr(x), len(x), _ptr(p), _ptr(out)))
         return out
+
+    def check_mesh(self):
+        """The device validator (g4d_check_mesh) on the last single-cloud
+        triangulation: dict of V, E, F, T, euler and the failure counts."""
+        r = CheckReport()
+        self._check(self._lib.g4d_check_mesh(self._h, ctypes.byref(r)))
+        return r.as_dict()
+
+    def check_tets(self, points, tets):
+        """The device validator on a given mesh (g4d_check_tets): points (n,3)
+        float64 and tets (structured TET_DTYPE, or (T, 8) int32)."""
+        pts = np.ascontiguousarray(points, dtype=np.float64)
+        t = np.asarray(tets)
+        if t.dtype != TET_DTYPE:
+            t = np.ascontiguousarray(t, dtype=np.int32).view(TET_DTYPE).reshape(-1)
+        t = np.ascontiguousarray(t)
+        r = CheckReport()
+        self._check(self._lib.g4d_check_tets(self._h, _ptr(pts), len(pts), _ptr(t), len(t), ctypes.byref(r)))
+        return r.as_dict()
 
     def mlp_wait_probe(self, limit):
         """Runs the tensor-core kernels' bounded wait on a phase nothing

@@ -70,7 +70,7 @@ enum BufId {
     B_WLEMIT, B_WLEMIT2, B_DROWN, B_DROWN2, B_CTR, B_CNT, B_BASE, B_TETS, B_CUB, B_BAD, B_LIDX, B_LHH, B_LTRI,
     B_WLINSL, B_WLPROM, B_SKEY0, B_SKEY, B_GIDX, B_LOCAL, B_BCKEY0, B_BCKEY, B_SLOTS, B_MMB, B_TC, B_TETS2, B_OVF, B_OVF2, B_KMASK, B_BOUT, B_OCC, B_WLEXACT, B_WLBIG,
     B_MLP_P, B_MLP_G, B_MLP_M1, B_MLP_M2, B_MLP_AUX, B_RING_PAIR, B_RING_X, B_RING_Y, B_RING_LOGIT, B_TILES,
-    B_DIAG_X, B_DIAG_Y, B_DIAG_P, B_DIAG_G, B_FIX, B_FACE, B_XYZ32, B_NUM
+    B_DIAG_X, B_DIAG_Y, B_DIAG_P, B_DIAG_G, B_FIX, B_FACE, B_XYZ32, B_CHECK, B_CHECKOUT, B_CHKP, B_CHKT, B_NUM
 };
 
 }  // namespace
@@ -106,6 +106,9 @@ struct g4d_ctx {
     std::vector<float> mlp;    // host copy of the parameters
     int ring_rows = 0;         // candidate rows of the last ring pass
     std::vector<int64_t> batch_offsets;  // tet offsets of the last device batch
+    // the tetrahedra in B_TETS belong to the last single-cloud call (not a batch)
+    bool has_result = false;
+    bool result_mapped = false;  // ... and use input indices (else Morton indices)
 };
 
 namespace {
@@ -605,6 +608,8 @@ g4d_status run_proposal(g4d_ctx* ctx, const Dev& D) {
 
 // Stages 2-5: digital Voronoi, stars, splaying, extraction.
 g4d_status run_compute(g4d_ctx* ctx, bool map_to_input) {
+    ctx->has_result = false;
+    ctx->result_mapped = map_to_input;
     Launch L{ctx->stream, &ctx->launches};
     const int n = ctx->n, G = ctx->G;
     const size_t G3 = (size_t)G * G * G;
@@ -646,7 +651,9 @@ g4d_status run_compute(g4d_ctx* ctx, bool map_to_input) {
     }
     st = run_splay(ctx, D);
     if (st) return st;
-    return run_extract(ctx, D, map_to_input ? ctx->b[B_ORDER].as<int>() : nullptr);
+    st = run_extract(ctx, D, map_to_input ? ctx->b[B_ORDER].as<int>() : nullptr);
+    ctx->has_result = st == G4D_OK;
+    return st;
 }
 
 void finish_stats(g4d_ctx* ctx) {
@@ -1023,6 +1030,7 @@ struct HostSink {
 
 g4d_status run_batch(g4d_ctx* ctx, const double* d_xyz, const int64_t* offs, int nclouds,
                      std::vector<int64_t>& counts, size_t* total, g4d_stats* acc, HostSink* sink = nullptr) {
+    ctx->has_result = false;
     for (int c = 0; c < nclouds; ++c) {
         const int64_t n = offs[c + 1] - offs[c];
         if (n < 5 || n >= (1 << 30))
@@ -1703,6 +1711,63 @@ g4d_status g4d_mlp_wait_probe(g4d_ctx* ctx, int limit) {
     CK_SYNC(ctx->stream);
     if (h.err) return fail(ctx, G4D_ERR_TIMEOUT, "tensor-core kernel wait ran out after %d polls (0x%x)", limit, h.err);
     return G4D_OK;
+}
+
+namespace {
+
+// the validator over points P (n, Morton order when order is given) and
+// device tetrahedra
+g4d_status check_on_device(g4d_ctx* ctx, const double4* P, const int* order, const g4d_tet* tets, int ntet, int n,
+                           g4d_check_report* report) {
+    CK(ctx->b[B_CHECK].ensure(check_scratch_bytes(ntet, n)));
+    CK(ctx->b[B_CHECKOUT].ensure(8 * sizeof(unsigned long long)));
+    unsigned long long* out = ctx->b[B_CHECKOUT].as<unsigned long long>();
+    unsigned* err = reinterpret_cast<unsigned*>(out + 6);
+    CK(cudaMemsetAsync(err, 0, sizeof(unsigned), ctx->stream));
+    CK(run_mesh_check(ctx->stream, &ctx->launches, P, order, tets, ntet, n, ctx->b[B_CHECK].p, out, err));
+    unsigned long long h[7] = {0, 0, 0, 0, 0, 0, 0};
+    CK(cudaMemcpyAsync(h, out, 7 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, ctx->stream));
+    CK_SYNC(ctx->stream);
+    const unsigned herr = (unsigned)h[6];
+    if (herr & 0x200u) return fail(ctx, G4D_ERR_INTERNAL, "a tetrahedron has a vertex index outside [0, %d)", n);
+    if (herr) return fail(ctx, G4D_ERR_PRECISION, "a validator predicate could not be evaluated exactly");
+    report->vertices = (long long)h[0];
+    report->edges = (long long)h[1];
+    report->triangles = (long long)h[2];
+    report->tets = ntet;
+    report->euler = report->vertices - report->edges + report->triangles - report->tets;
+    report->orient_fail = (long long)h[3];
+    report->insphere_fail = (long long)h[4];
+    report->adjacency_fail = (long long)h[5];
+    return G4D_OK;
+}
+
+}  // namespace
+
+g4d_status g4d_check_mesh(g4d_ctx* ctx, g4d_check_report* report) {
+    if (!ctx || !report) return G4D_ERR_ARG;
+    if (!ctx->has_result) return fail(ctx, G4D_ERR_ARG, "no single-cloud triangulation to check");
+    cudaSetDevice(ctx->device);
+    return check_on_device(ctx, ctx->b[B_P].as<double4>(), ctx->result_mapped ? ctx->b[B_ORDER].as<int>() : nullptr,
+                           ctx->b[B_TETS].as<g4d_tet>(), ctx->ntet, ctx->n, report);
+}
+
+g4d_status g4d_check_tets(g4d_ctx* ctx, const double* xyz, int n, const g4d_tet* tets, int ntet,
+                          g4d_check_report* report) {
+    if (!ctx || !xyz || !report || n < 1 || ntet < 0 || (ntet > 0 && !tets)) return G4D_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    std::vector<double4> p((size_t)n);
+    for (int i = 0; i < n; ++i) p[i] = make_double4(xyz[3 * (size_t)i], xyz[3 * (size_t)i + 1], xyz[3 * (size_t)i + 2], 0.0);
+    CK(ctx->b[B_CHKP].ensure(sizeof(double4) * (size_t)n));
+    CK(ctx->b[B_CHKT].ensure(sizeof(g4d_tet) * (size_t)std::max(ntet, 1)));
+    CK(cudaMemcpyAsync(ctx->b[B_CHKP].p, p.data(), sizeof(double4) * (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
+    if (ntet)
+        CK(cudaMemcpyAsync(ctx->b[B_CHKT].p, tets, sizeof(g4d_tet) * (size_t)ntet, cudaMemcpyHostToDevice,
+                           ctx->stream));
+    g4d_status st = check_on_device(ctx, ctx->b[B_CHKP].as<double4>(), nullptr, ctx->b[B_CHKT].as<g4d_tet>(), ntet,
+                                    n, report);
+    CK_SYNC(ctx->stream);  // the host copy of the points outlives the upload
+    return st;
 }
 
 void* g4d_stream(g4d_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }

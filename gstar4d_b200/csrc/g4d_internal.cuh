@@ -300,6 +300,11 @@ void launch_ring(const Launch& L, const Dev& D, const Ring& R);
 void launch_ring_labels(const Launch& L, const Dev& D, const int2* pair, const int* rows, int cap, float* y);
 void launch_prop_merge(const Launch& L, const Dev& D, const int2* pair, const float* logits, const int* rows,
                        int cap, float threshold);
+// mesh validator (g4d_check.cu)
+size_t check_scratch_bytes(int ntet, int n);
+cudaError_t run_mesh_check(cudaStream_t st, long long* launches, const double4* P, const int* order,
+                           const g4d_tet* tets, int ntet, int n, void* scratch, unsigned long long* out,
+                           unsigned* err);
 void launch_eval_pred(const Launch& L, int kind, const double* pts, const int* idx, int count, int8_t* out,
                       unsigned* err);
 

@@ -239,6 +239,28 @@ G4D_API g4d_status g4d_mlp_infer(g4d_ctx* ctx, const uint16_t* x, int m, const f
  * context stays usable (the path a real timeout of an MLP kernel takes). */
 G4D_API g4d_status g4d_mlp_wait_probe(g4d_ctx* ctx, int limit);
 
+/* Counts of the mesh validator (TetraMesh::check, Common/Geometry.cu:200-393). */
+typedef struct {
+    long long vertices, edges, triangles, tets;  /* distinct V, E, F; T */
+    long long euler;                             /* V - E + F - T: 1 for a triangulated ball */
+    long long orient_fail;                       /* tetrahedra with orient3d(v0, v1, v2, v3) > 0 */
+    long long insphere_fail;                     /* interior faces with insphere(tet, opposite vertex) < 0 */
+    long long adjacency_fail;                    /* opp links out of range or not reciprocated */
+} g4d_check_report;
+
+/* The -check validator on the device: the reference's Euler, orientation and
+ * in-sphere checks (Common/Geometry.cu:200-393) over the tetrahedra of the
+ * context's last single-cloud triangulation (g4d_triangulate*, or
+ * g4d_gdel_compute), with exact orient3d and insphere signs and no Simulation
+ * of Simplicity, as the reference's validator computes them. Fills *report;
+ * a valid Delaunay mesh has euler == 1 and every failure count 0. */
+G4D_API g4d_status g4d_check_mesh(g4d_ctx* ctx, g4d_check_report* report);
+/* The same validator on a caller's mesh: xyz (n*3 doubles, host) and tets
+ * (ntet tetrahedra indexing xyz, host). Vertex and neighbour indices out of
+ * range are counted, never followed. */
+G4D_API g4d_status g4d_check_tets(g4d_ctx* ctx, const double* xyz, int n, const g4d_tet* tets, int ntet,
+                                  g4d_check_report* report);
+
 /* The command line's point generator: Application::makePoints
  * (Main/Application.cpp:316-473) with its KISS random numbers (DtRandom,
  * Common/DtRandom.cpp:44-109, unsigned long = 64 bits as on Linux). Writes n

@@ -37,15 +37,17 @@ def test_read_points_drops_duplicates(tmp_path):
     assert p.tolist() == [[0, 0, 0], [1, 2, 3], [4, 5, 6]]
 
 
-def test_ply_layout_and_adjacency_check(tmp_path):
+def test_ply_layout_and_check_report(tmp_path, capsys):
     from gstar4d_b200.api import TET_DTYPE
     pts = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1], [1, 1, 1]], float)
     t = np.zeros(2, TET_DTYPE)
     t["v"] = [[0, 1, 2, 3], [1, 2, 3, 4]]
     t["opp"] = [[1, -1, -1, -1], [-1, -1, -1, 0]]
-    assert cli.check_adjacency(t) == 0
-    t["opp"][0, 0] = -1
-    assert cli.check_adjacency(t) == 1
+    ok = dict(vertices=5, edges=9, triangles=7, tets=2, euler=1, orient_fail=0, insphere_fail=0, adjacency_fail=0)
+    assert cli.print_check(ok)
+    assert "Tetra in-sphere is correct!" in capsys.readouterr().out
+    assert not cli.print_check(dict(ok, insphere_fail=3))
+    assert "In-sphere check failed!!!" in capsys.readouterr().out
     f = tmp_path / "m.ply"
     cli.write_ply(str(f), pts, t)
     lines = f.read_text().splitlines()

@@ -19,13 +19,25 @@ def test_generated_points_run_check_and_files(tmp_path, capsys, monkeypatch):
     assert "Seed: 3" in out and "Seed: 4" in out
     for label in ("Init:", "PBA:", "InitStar:", "Consistency:", "StarOutput:", "Total Time:"):
         assert out.count(label) == 2
-    assert out.count("adjacency OK") == 2
+    assert out.count("Tetra orientation is correct!") == 2 and out.count("Tetra in-sphere is correct!") == 2
+    assert out.count("Euler: 1\n") == 2
     assert os.path.exists("mesh.ply") and os.path.exists("Input-Points.asc")
     assert len(open("Input-Points.asc").read().splitlines()) == 3000
     t = open("gStar4D-time.txt").read().splitlines()
     c = open("gStar4D-count.txt").read().splitlines()
     assert len(t) == 1 and t[0].startswith("GridSize,64,Runs,2,Points,3000,Input,Gaussian,Total Time,")
     assert len(c) == 1 and ",Loop number," in c[0]
+
+
+def test_generated_points_are_the_reference_clis(tmp_path, monkeypatch):
+    """-n -g -d -s give the reference command line's points (its KISS
+    generator restated in C++; pinned to the reference code in
+    tests/test_ref_pins.py)."""
+    monkeypatch.chdir(tmp_path)
+    assert cli.main(["-n", "2000", "-g", "128", "-s", "9", "-d", "3", "-outFile", "m.ply"]) == 0
+    pts = np.loadtxt("Input-Points.asc")
+    from gstar4d_b200 import api
+    assert np.allclose(pts, api.make_points(2000, 128, 3, 9), rtol=1e-5, atol=1e-3)  # 6 significant digits
 
 
 def test_file_input_is_scaled_and_triangulated(tmp_path, capsys, monkeypatch):
@@ -36,6 +48,6 @@ def test_file_input_is_scaled_and_triangulated(tmp_path, capsys, monkeypatch):
     rc = cli.main(["-inFile", "in.txt", "-g", "64", "-check", "-outFile", "m.ply"])
     assert rc == 0
     out = capsys.readouterr().out
-    assert "5 duplicate points in input file!" in out and "adjacency OK" in out
+    assert "5 duplicate points in input file!" in out and "Tetra in-sphere is correct!" in out
     s = np.loadtxt("Input-Scaled-Points.asc")
     assert len(s) == 2000 and s.min() >= 1.0 - 1e-4 and s.max() <= 62.0 + 1e-4
