@@ -163,16 +163,17 @@ def log_lines(o, n, sums):
 
 
 def write_ply(path, points, tets):
-    """The reference's TetraMesh::writeToFile layout (Geometry.cu:396-460):
-    ASCII PLY, the vertices, then three faces per tetrahedron."""
+    """The reference's TetraMesh::writeToFile (Geometry.cu:396-466): ASCII PLY,
+    each vertex as its coordinates in the stream's default format (%g) each
+    followed by a space, then three faces per tetrahedron, tetrahedron by
+    tetrahedron: (v0 v1 v2), (v0 v1 v3), (v0 v2 v3)."""
     v = np.asarray(tets["v"] if getattr(tets, "dtype", None) is not None and tets.dtype.names else tets)[:, :4]
-    faces = np.concatenate([v[:, [0, 1, 2]], v[:, [0, 1, 3]], v[:, [0, 2, 3]]], axis=0) if len(v) else np.zeros(
-        (0, 3), np.int64)
     with open(path, "w") as f:
         f.write("ply\nformat ascii 1.0\nelement vertex %d\nproperty float x\nproperty float y\nproperty float z\n"
-                "element face %d\nproperty list uchar int vertex_index\nend_header\n" % (len(points), len(faces)))
-        np.savetxt(f, points, fmt="%.9g")
-        np.savetxt(f, np.concatenate([np.full((len(faces), 1), 3), faces], axis=1), fmt="%d")
+                "element face %d\nproperty list uchar int vertex_index\nend_header\n" % (len(points), 3 * len(v)))
+        f.write("".join("%g %g %g \n" % (p[0], p[1], p[2]) for p in np.asarray(points, np.float64)))
+        f.write("".join("3 %d %d %d \n3 %d %d %d \n3 %d %d %d \n" % (t[0], t[1], t[2], t[0], t[1], t[3], t[0], t[2], t[3])
+                        for t in v.tolist()))
 
 
 def print_check(rep):

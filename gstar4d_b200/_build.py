@@ -1,6 +1,7 @@
-"""Builds the CUDA library gstar4d_b200/libgstar4d.so for sm_100a with nvcc.
+"""Builds the CUDA library gstar4d_b200/libgstar4d.so for sm_100a with nvcc,
+and the native command line gstar4d_b200/gstar4d over its C ABI.
 
-The .so is built in-tree so that it travels with the repository to the GPU
+Both are built in-tree so that they travel with the repository to the GPU
 host; nothing is installed into site-packages.
 """
 import os
@@ -13,12 +14,20 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgstar4d.so")
+EXE = os.path.join(HERE, "gstar4d")  # native command line
 OBJ = os.path.join(HERE, "_build")
 
 SOURCES = ["g4d_order.cu", "g4d_pba.cu", "g4d_star.cu", "g4d_api.cu", "g4d_noalloc.cu", "g4d_mlp.cu", "g4d_proposal.cu", "g4d_check.cu", "g4d_points.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
          "-I", os.path.join(REPO, "include"), "-I", CSRC, "--expt-relaxed-constexpr"]
+
+
+def _cxx():
+    for cand in (os.environ.get("CXX"), "/usr/bin/g++", shutil.which("g++")):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("g++ not found")
 
 
 def _nvcc():
@@ -29,9 +38,9 @@ def _nvcc():
 
 
 def _stale():
-    if not os.path.exists(LIB):
+    if not os.path.exists(LIB) or not os.path.exists(EXE):
         return True
-    t = os.path.getmtime(LIB)
+    t = min(os.path.getmtime(LIB), os.path.getmtime(EXE))
     deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(REPO, "include", "gstar4d.h")]
     return any(os.path.getmtime(d) > t for d in deps)
 
@@ -64,6 +73,12 @@ def build(force=False, verbose=False):
     tmp = LIB + ".tmp"
     subprocess.check_call([nvcc] + ARCH + ["-shared", "-o", tmp] + objs + ["-lcudart"])
     os.replace(tmp, LIB)
+    # the native command line over the C ABI, next to the library it loads
+    tmp = EXE + ".tmp"
+    subprocess.check_call([_cxx(), "-O2", "-std=c++17", "-I", os.path.join(REPO, "include"),
+                           os.path.join(CSRC, "gstar4d_cli.cpp"), "-o", tmp, "-L", HERE, "-lgstar4d",
+                           "-Wl,-rpath,$ORIGIN"])
+    os.replace(tmp, EXE)
     return LIB
 
 

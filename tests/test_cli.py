@@ -52,7 +52,10 @@ def test_ply_layout_and_check_report(tmp_path, capsys):
     cli.write_ply(str(f), pts, t)
     lines = f.read_text().splitlines()
     assert lines[0] == "ply" and "element vertex 5" in lines and "element face 6" in lines
-    assert lines[lines.index("end_header") + 6] == "3 0 1 2"
+    h = lines.index("end_header")
+    # TetraMesh::writeToFile: "x y z " per vertex, three faces per tetrahedron in turn
+    assert lines[h + 1] == "0 0 0 " and lines[h + 5] == "1 1 1 "
+    assert lines[h + 6:h + 12] == ["3 0 1 2 ", "3 0 1 3 ", "3 0 2 3 ", "3 1 2 3 ", "3 1 2 4 ", "3 1 3 4 "]
 
 
 def test_float_flag_rounds_points_to_float32(tmp_path):

@@ -51,3 +51,55 @@ def test_file_input_is_scaled_and_triangulated(tmp_path, capsys, monkeypatch):
     assert "5 duplicate points in input file!" in out and "Tetra in-sphere is correct!" in out
     s = np.loadtxt("Input-Scaled-Points.asc")
     assert len(s) == 2000 and s.min() >= 1.0 - 1e-4 and s.max() <= 62.0 + 1e-4
+
+
+def _ply(path):
+    """(header and vertex lines, sorted tetrahedra) of a mesh written in
+    TetraMesh::writeToFile's layout; the tetrahedron order of two runs may
+    differ (insertion order on the device is not fixed), the set may not."""
+    lines = path.read_text().splitlines()
+    h = lines.index("end_header")
+    nv = int(next(ln for ln in lines if ln.startswith("element vertex")).split()[2])
+    faces = [list(map(int, ln.split()[1:])) for ln in lines[h + 1 + nv:]]
+    tets = sorted(tuple(sorted(f0 + [f1[2]])) for f0, f1 in zip(faces[0::3], faces[1::3]))
+    return lines[:h + 1 + nv], tets
+
+
+def test_native_command_line_matches_the_python_one(tmp_path, monkeypatch):
+    """The native executable (gstar4d_b200/gstar4d, C++ over the C ABI) and
+    the Python command line write the same PLY mesh and input points for the
+    same flags, generated and file input, and its -check passes."""
+    import subprocess
+    exe = os.path.join(os.path.dirname(cli.__file__), "gstar4d")
+    assert os.path.exists(exe)
+    for args in (["-n", "4000", "-g", "64", "-s", "2", "-d", "0"], ["-n", "3000", "-g", "128", "-s", "5", "-d", "3"]):
+        for tool in ("native", "python"):
+            d = tmp_path / (tool + "_" + args[5])
+            d.mkdir()
+            monkeypatch.chdir(d)
+            if tool == "native":
+                r = subprocess.run([exe] + args + ["-check", "-outFile", "m.ply"], capture_output=True, text=True)
+                assert r.returncode == 0, r.stdout + r.stderr
+                assert "Tetra in-sphere is correct!" in r.stdout and "Euler: 1" in r.stdout
+            else:
+                assert cli.main(args + ["-outFile", "m.ply"]) == 0
+        a, b = tmp_path / ("native_" + args[5]), tmp_path / ("python_" + args[5])
+        assert _ply(a / "m.ply") == _ply(b / "m.ply")
+        assert (a / "Input-Points.asc").read_bytes() == (b / "Input-Points.asc").read_bytes()
+    # file input, double and float scaling
+    pts = np.random.default_rng(6).random((1500, 3)) * 7.0 - 2.0
+    src = tmp_path / "in.txt"
+    np.savetxt(src, pts, fmt="%.8g")
+    for extra in ([], ["-float"]):
+        outs = []
+        for tool in ("native", "python"):
+            d = tmp_path / ("file_" + tool + "_" + str(len(extra)))
+            d.mkdir()
+            monkeypatch.chdir(d)
+            args = ["-inFile", str(src), "-g", "64", "-outFile", "m.ply"] + extra
+            if tool == "native":
+                assert subprocess.run([exe] + args, capture_output=True).returncode == 0
+            else:
+                assert cli.main(args) == 0
+            outs.append((_ply(d / "m.ply"), (d / "Input-Scaled-Points.asc").read_bytes()))
+        assert outs[0] == outs[1]
