@@ -431,9 +431,13 @@ def main():
     # same configuration with labels from the plain method, then timed like value
     learned = None
     if not args.no_learned:
-        train_pts, _ = workloads.config_cloud(args.workload, scale=args.points / base_points,
+        # features are in voxel units, so a 1/8-size cloud of the configuration
+        # at half the grid width (the same voxel density) trains as well and
+        # 8x faster
+        small = args.grid >= 256 and args.points >= 800_000
+        train_pts, _ = workloads.config_cloud(args.workload, scale=args.points / base_points / (8 if small else 1),
                                               seed=cfg["seed"] + 1000 + rank)
-        with gstar4d_b200.Triangulator(grid_size=args.grid, device=local) as tt:
+        with gstar4d_b200.Triangulator(grid_size=args.grid // 2 if small else args.grid, device=local) as tt:
             t0 = time.perf_counter()
             loss = tt.train_proposal(train_pts, epochs=4, lr=2e-3)
             train_s = time.perf_counter() - t0
@@ -463,7 +467,9 @@ def main():
                    "splay_insertions_per_point": round(stl["splay_insertions"] / n, 3),
                    "proposed_per_point": round(stl["proposed"] / n, 3), "loops": stl["loops"],
                    "stages_ms": {k: round(stl[k], 3) for k in ("t_pba_ms", "t_star_ms", "t_splay_ms", "t_out_ms")},
-                   "training": {"cloud": "same configuration, seed + 1000", "epochs": 4,
+                   "training": {"cloud": ("1/8-size cloud of the same configuration, seed + 1000, at half the grid "
+                                          "width (same voxel density)") if small else
+                                         "same configuration, seed + 1000", "epochs": 4,
                                 "final_loss": round(loss, 4), "seconds": round(train_s, 2)}}
         tl.close()
 

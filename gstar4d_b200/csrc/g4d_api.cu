@@ -98,7 +98,9 @@ struct g4d_ctx {
     std::vector<double> gdel_points;
     bool gdel_ready = false;
     cudaEvent_t ev[8];
+    cudaEvent_t tune_ev[2] = {nullptr, nullptr};  // the PBA form tuner's own timing events
     std::map<int, int> tuned;  // autotuner: (size bucket, distribution class) -> grid width
+    std::map<int, int> pba_form;  // autotuner: grid width -> fastest PBA pass form
     int next_grid = 0;         // tuned width for the next single-cloud call (0: none)
     // learned star proposal
     bool has_model = false;
@@ -606,6 +608,39 @@ g4d_status run_proposal(g4d_ctx* ctx, const Dev& D) {
     return G4D_OK;
 }
 
+// The y and x passes in the form tuned for this grid width: the first grid
+// of a width on a context times every form (the z pass rebuilds the input
+// before each, since the line form uses it as scratch) and keeps the fastest;
+// later grids of that width use it. All forms give exact distances.
+// G4D_PBA_FORM=<0..2> in the environment at context creation fixes the form.
+int pba_form_for(g4d_ctx* ctx, const Dev& D, uint32_t* gA, uint32_t* gB) {
+    const int G = D.G;
+    if (ctx->pba_form.count(G)) return ctx->pba_form[G];
+    Launch L{ctx->stream, &ctx->launches};
+    cudaEvent_t a = ctx->tune_ev[0], b = ctx->tune_ev[1];
+    int best = pba_default_form(G);
+    float best_ms = 1e30f;
+    for (int f = 0; f < PBA_FORMS; ++f) {
+        if (!pba_form_ok(f, G)) continue;
+        float ms = 0.f;
+        for (int rep = 0; rep < 2; ++rep) {  // the first run of a form also loads its kernels
+            launch_pba_z(L, D, gA);
+            cudaEventRecord(a, ctx->stream);
+            launch_pba_y(L, G, gA, gB, f);
+            launch_pba_x(L, G, gB, gA, f);
+            cudaEventRecord(b, ctx->stream);
+            if (cudaEventSynchronize(b) != cudaSuccess) return best;
+            cudaEventElapsedTime(&ms, a, b);
+        }
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = f;
+        }
+    }
+    ctx->pba_form[G] = best;
+    return best;
+}
+
 // Stages 2-5: digital Voronoi, stars, splaying, extraction.
 g4d_status run_compute(g4d_ctx* ctx, bool map_to_input) {
     ctx->has_result = false;
@@ -621,13 +656,14 @@ g4d_status run_compute(g4d_ctx* ctx, bool map_to_input) {
     // equalise the two drowned buffers' capacity
     D.drownCap = (int)std::min(ctx->b[B_DROWN].cap, ctx->b[B_DROWN2].cap) / (int)sizeof(int2);
 
-    cudaEventRecord(ctx->ev[1], ctx->stream);
-    // digital Voronoi diagram
     uint32_t* gA = ctx->b[B_GA].as<uint32_t>();
     uint32_t* gB = ctx->b[B_GB].as<uint32_t>();
+    const int form = pba_form_for(ctx, D, gA, gB);
+    cudaEventRecord(ctx->ev[1], ctx->stream);
+    // digital Voronoi diagram
     launch_pba_z(L, D, gA);
-    launch_pba_y(L, G, gA, gB);
-    launch_pba_x(L, G, gB, gA);
+    launch_pba_y(L, G, gA, gB, form);
+    launch_pba_x(L, G, gB, gA, form);
     cudaEventRecord(ctx->ev[2], ctx->stream);
     // worksets (repeated with a longer overflow list if theirs ran out)
     for (int attempt = 0;; ++attempt) {
@@ -850,8 +886,10 @@ g4d_status run_wave(g4d_ctx* ctx, const double* d_xyz, const int64_t* offs, cons
     uint32_t* gB = ctx->b[B_GB].as<uint32_t>();
     for (const Stack& S : stacks) {
         launch_pba_z_stack(L, S.G, S.K, ckey, cs + S.col, ce + S.col, gA + S.vox);
-        launch_pba_y_stack(L, S.G, S.K, gA + S.vox, gB + S.vox);
-        launch_pba_x_stack(L, S.G, S.K, gB + S.vox, gA + S.vox);
+        const auto tf = ctx->pba_form.find(S.G);  // a width tuned on single clouds, else the default
+        const int form = tf != ctx->pba_form.end() ? tf->second : -1;
+        launch_pba_y_stack(L, S.G, S.K, gA + S.vox, gB + S.vox, form);
+        launch_pba_x_stack(L, S.G, S.K, gB + S.vox, gA + S.vox, form);
     }
     cudaEventRecord(ctx->ev[2], ctx->stream);
     for (int attempt = 0;; ++attempt) {
@@ -1180,6 +1218,12 @@ g4d_status g4d_create(g4d_ctx** out, const g4d_config* cfg) {
         return G4D_ERR_CUDA;
     }
     for (auto& e : ctx->ev) cudaEventCreate(&e);
+    for (auto& e : ctx->tune_ev) cudaEventCreate(&e);
+    if (const char* f = std::getenv("G4D_PBA_FORM")) {
+        const int form = std::atoi(f);
+        for (int G = 32; G <= 1024; G *= 2)
+            if (pba_form_ok(form, G)) ctx->pba_form[G] = form;
+    }
     if (const char* f = std::getenv("G4D_FAIL_ALLOC_AFTER")) {
         ctx->budget.left = std::atoll(f);
         for (auto& b : ctx->b) b.budget = &ctx->budget;
@@ -1196,6 +1240,8 @@ void g4d_destroy(g4d_ctx* ctx) {
     if (ctx->side) cudaStreamSynchronize(ctx->side);
     for (auto& b : ctx->b) b.release();
     for (auto& e : ctx->ev) cudaEventDestroy(e);
+    for (auto& e : ctx->tune_ev)
+        if (e) cudaEventDestroy(e);
     if (ctx->fork) cudaEventDestroy(ctx->fork);
     if (ctx->join) cudaEventDestroy(ctx->join);
     if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
@@ -1525,9 +1571,11 @@ g4d_status g4d_voronoi(g4d_ctx* ctx, const double* xyz, int n, int grid, uint32_
     CK(ctx->b[B_GB].ensure(sizeof(uint32_t) * G3));
     Launch L{ctx->stream, &ctx->launches};
     Dev D = make_dev(ctx);
+    const auto tf = ctx->pba_form.find(grid);  // a tuned (or fixed) form for this width, else the default
+    const int form = tf != ctx->pba_form.end() ? tf->second : -1;
     launch_pba_z(L, D, ctx->b[B_GA].as<uint32_t>());
-    launch_pba_y(L, grid, ctx->b[B_GA].as<uint32_t>(), ctx->b[B_GB].as<uint32_t>());
-    launch_pba_x(L, grid, ctx->b[B_GB].as<uint32_t>(), ctx->b[B_GA].as<uint32_t>());
+    launch_pba_y(L, grid, ctx->b[B_GA].as<uint32_t>(), ctx->b[B_GB].as<uint32_t>(), form);
+    launch_pba_x(L, grid, ctx->b[B_GB].as<uint32_t>(), ctx->b[B_GA].as<uint32_t>(), form);
     CK(cudaMemcpyAsync(sites, ctx->b[B_GA].p, sizeof(uint32_t) * G3, cudaMemcpyDeviceToHost, ctx->stream));
     unsigned herr = 0;
     CK(cudaMemcpyAsync(&herr, &ctx->b[B_CTR].as<Counters>()->err, sizeof(unsigned), cudaMemcpyDeviceToHost,

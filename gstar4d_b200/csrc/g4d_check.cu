@@ -14,8 +14,8 @@
 // orient3d and insphere are the exact signs of Shewchuk's predicates (the
 // filter and exact stages of g4d_predicates.cuh, no Simulation of Simplicity,
 // as in the reference's validator). A neighbour index out of range, or a
-// neighbour that does not link back, counts as an adjacency failure (the
-// reference asserts on it).
+// neighbour that does not link back (checked from both sides), counts as an
+// adjacency failure (the reference asserts on it).
 #include <cub/cub.cuh>
 
 #include "g4d_internal.cuh"
@@ -154,7 +154,8 @@ __global__ void k_chk_geometry(const double4* __restrict__ P, const int* __restr
                 atomicAdd(&counts[2], 1ull);
                 continue;
             }
-            if (t > o) continue;  // each pair once, from the smaller index
+            // every link must come back; the in-sphere test runs once per
+            // pair, from the smaller index
             const g4d_tet U = tets[o];
             int k = -1;
             for (int j = 0; j < 4; ++j)
@@ -163,6 +164,7 @@ __global__ void k_chk_geometry(const double4* __restrict__ P, const int* __restr
                 atomicAdd(&counts[2], 1ull);
                 continue;
             }
+            if (t > o) continue;
             q[4] = pt(P, inv, U.v[k]);
             if (insphere_sign(q, err) < 0) atomicAdd(&counts[1], 1ull);
         }

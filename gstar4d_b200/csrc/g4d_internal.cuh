@@ -241,9 +241,18 @@ void launch_b_localize(const Launch& L, const g4d_tet* in, int ntet, const unsig
                        const int* local, const int* base, const int* slotW, const long long* dst, g4d_tet* out);
 
 // pba
+// Forms of the y and x passes (g4d_pba.cu): one thread per line, or lines
+// staged in shared memory in tiles (4 lines per warp in both passes, 4 warps
+// per block; or 2 lines per warp in the x pass, 2 warps per block). Their
+// outputs are equally exact; which is fastest depends on the grid width, so
+// contexts time them on the first grid of each width (g4d_api.cu).
+enum PbaForm : int { PBA_LINES = 0, PBA_TILES_4 = 1, PBA_TILES_2 = 2, PBA_FORMS = 3 };
+int pba_default_form(int G);
+bool pba_form_ok(int form, int G);
 void launch_pba_z(const Launch& L, const Dev& D, uint32_t* out);
-void launch_pba_y(const Launch& L, int G, uint32_t* in, uint32_t* out);
-void launch_pba_x(const Launch& L, int G, uint32_t* in, uint32_t* out);
+// `in` is scratch (the line form keeps its stacks in it); form -1: the default
+void launch_pba_y(const Launch& L, int G, uint32_t* in, uint32_t* out, int form = -1);
+void launch_pba_x(const Launch& L, int G, uint32_t* in, uint32_t* out, int form = -1);
 void launch_pairs(const Launch& L, const Dev& D, const uint32_t* grid, int* map);
 void launch_site_map(const Launch& L, const Dev& D, int* map);
 void launch_b_site_map(const Launch& L, const uint32_t* vox, const unsigned long long* skey, const int* slotG,
@@ -252,8 +261,8 @@ void launch_missing(const Launch& L, const Dev& D);
 // stacks of K grids of width G (batches; 64-bit column keys)
 void launch_pba_z_stack(const Launch& L, int G, int K, const unsigned long long* ckey, const int* cs, const int* ce,
                         uint32_t* out);
-void launch_pba_y_stack(const Launch& L, int G, int K, uint32_t* in, uint32_t* out);
-void launch_pba_x_stack(const Launch& L, int G, int K, uint32_t* in, uint32_t* out);
+void launch_pba_y_stack(const Launch& L, int G, int K, uint32_t* in, uint32_t* out, int form = -1);
+void launch_pba_x_stack(const Launch& L, int G, int K, uint32_t* in, uint32_t* out, int form = -1);
 void launch_pairs_stack(const Launch& L, const Dev& D, const uint32_t* stack, int* map, int G, int K,
                         const unsigned long long* ckey, const int* cid, const int* cs, const int* ce);
 void launch_missing_u64(const Launch& L, const Dev& D, const unsigned long long* mkey);

@@ -8,9 +8,9 @@
 // phases are re-planned for B200:
 //   z: seeding fused with the flood. Sites are bucketed per (x,y) column by a
 //      radix sort, so each column is written once (4 B/voxel, no memset, no read).
-//   y, x: one thread per line builds the lower envelope of the line's
-//      candidates and colours the line from it (O(G) per line, no transposes;
-//      k_pba_env_y / k_pba_env_x below).
+//   y, x: tiles of 8 lines staged in shared memory, one warp per line
+//      building the line's lower envelope from 32 band hulls merged in a tree
+//      and colouring the line from it (k_pba_env below; no transposes).
 // Sites stay encoded as voxel coordinates; the pair scan turns them into point
 // ids through a voxel -> leader map written into the free second grid.
 //
@@ -58,29 +58,348 @@ __global__ void __launch_bounds__(128) k_pba_z(int G, const KeyT* __restrict__ c
 
 
 // ---------------------------------------------------------------------------
-// y and x passes as lower envelopes (one thread per line, O(G) per line).
+// y and x passes: the exact 1D lower envelope of every line, on tiles of lines
+// staged in shared memory.
 //
 // Along a line, candidate p (a voxel whose site came from the earlier passes)
 // gives every voxel q the squared distance (q - p)^2 + f_p, f_p the squared
 // distance of its site across the line. The nearest site of each voxel is the
-// lowest of these parabolas: the lower convex hull of the points
-// (p, F_p = f_p + p^2), built in one sweep with a stack (Felzenszwalb and
-// Huttenlocher's envelope, the role of PBA's proximate-site stacks,
-// pba3DKernel.h:200-420), then read off in a second sweep. The sweep goes
-// downwards, so the stack is a list linked towards larger p; its links are
-// written into the input word of each stacked candidate (the input is
-// scratch), packed with the site coordinates the line does not fix. The
-// colouring sweep goes upwards along those links. Each thread keeps the two
-// top entries in registers, so a pop costs one load (of the new second).
-// Distances are exact; among equidistant sites the choice is free (only the
-// distance of the digital diagram is specified).
+// lowest of these parabolas, i.e. the lower convex hull of the points
+// (p, F_p = f_p + p^2) (Felzenszwalb and Huttenlocher's envelope; PBA's
+// proximate-site stacks and band merge, pba3DKernel.h:200-420, compute the
+// same hull). Each warp stages LPW whole lines in shared memory (one coalesced
+// read of every voxel) and splits every line into B = 32 / LPW bands, one lane
+// per band:
+//  1. lane (line i, band b) builds the hull of its band left to right, with
+//     the stack kept in place in the staged words;
+//  2. the bands of a line are merged pairwise in log2(B) levels, each merge by
+//     one lane walking to the lower common tangent of the two chains and
+//     cutting them there (every walk step removes a point; with B <= 8 the
+//     walks are a few steps, measured on the benchmark clouds);
+//  3. lane (i, b) colours its band: a binary search over the surviving hull
+//     points (addressed by rank through the bands' surviving runs) finds the
+//     point nearest to the band's first voxel, since the distance to a fixed
+//     voxel is convex along the hull (no division), then it walks forward,
+//     writing each site straight to the output (the y pass with 8 lines per
+//     warp: 8 consecutive x, one 32-byte sector per band per store; the x pass:
+//     4 sites per 16-byte store).
+// The words are site voxels, and the position of a candidate along the line is
+// one of its own coordinates (y in the y pass, x in the x pass), so the hull
+// holds words only. Distances are exact; among equidistant sites the choice is
+// free (only the distance of the digital diagram is specified); collinear hull
+// points are dropped.
 // ---------------------------------------------------------------------------
-constexpr uint32_t ENV_END = 2047;  // end of a list (11-bit link)
 
-// Products of height differences (< 3 G^2) and position differences (< G):
+// Products of height differences (< 4 G^2) and position differences (< G):
 // 32-bit up to G = 512, 64-bit beyond.
 template <bool WIDE>
 using EnvInt = typename std::conditional<WIDE, long long, int>::type;
+
+template <int AXIS>
+struct EnvLine {
+    int a, b;  // the line's fixed coordinates: (x, z) for the y pass (AXIS 1), (y, z) for the x pass (AXIS 0)
+    __device__ __forceinline__ int pos(uint32_t w) const { return AXIS ? (int)vy(w) : (int)vx(w); }
+    __device__ __forceinline__ int f(uint32_t w) const {
+        const int dz = b - (int)vz(w);
+        if (AXIS) return dz * dz;
+        const int dy = a - (int)vy(w);
+        return dy * dy + dz * dz;
+    }
+    __device__ __forceinline__ int height(uint32_t w) const { const int p = pos(w); return f(w) + p * p; }
+    __device__ __forceinline__ int dist(int q, uint32_t w) const { const int d = q - pos(w); return d * d + f(w); }
+};
+
+// (pb - pa)(Fc - Fa) - (Fb - Fa)(pc - pa) > 0: b lies strictly below the
+// segment from a to c (positions pa < pb < pc)
+template <bool WIDE>
+__device__ __forceinline__ bool below(int pa, int Fa, int pb, int Fb, int pc, int Fc) {
+    using I = EnvInt<WIDE>;
+    return (I)(pb - pa) * (I)(Fc - Fa) - (I)(Fb - Fa) * (I)(pc - pa) > 0;
+}
+
+// Staged line layout: band b of a line at word b (Lb + 1) (one padding word
+// per band), lines S = G + B words apart. With Lb a multiple of 32 the 32
+// lanes of a warp, one per (line, band), read 32 different banks.
+template <int LPW>
+struct EnvTile {
+    static constexpr int B = 32 / LPW;
+    int Lb, S;
+    __device__ __forceinline__ int idx(int q) const { return q + q / Lb; }  // position -> word within the line
+};
+
+template <int LPW>
+__host__ __device__ constexpr size_t env_warp_smem(int G) {
+    return (size_t)LPW * (size_t)(G + 32 / LPW) * 4 + (size_t)LPW * (32 / LPW) * 2 * 4;
+}
+
+// The envelope of the LPW lines staged in A (line i at A + i S), colouring
+// written through emit(i, q, site) for q = 0 .. G-1 of each band in turn.
+template <int AXIS, bool WIDE, int LPW, class Emit>
+__device__ __forceinline__ void env_lines(int G, const EnvTile<LPW>& T, uint32_t* A, int* lo, int* hi, int l0,
+                                          int c1, Emit& emit) {
+    constexpr int B = EnvTile<LPW>::B;
+    const int lane = threadIdx.x & 31;
+    const int i = lane % LPW, b = lane / LPW;
+    const int Lb = T.Lb;
+    uint32_t* line = A + i * T.S;
+    int* lo_i = lo + i * B;
+    int* hi_i = hi + i * B;
+    const EnvLine<AXIS> ln{l0 + i, c1};
+    // 1. the hull of this lane's band, in place
+    {
+        uint32_t* band = line + b * (Lb + 1);
+        int cnt = 0, ps = 0, Fs = 0, pt = 0, Ft = 0;
+        for (int k = 0; k < Lb; ++k) {
+            const uint32_t w = band[k];
+            if (w == MARKER) continue;
+            const int p = ln.pos(w), F = ln.height(w);
+            while (cnt >= 2 && !below<WIDE>(ps, Fs, pt, Ft, p, F)) {
+                --cnt;
+                pt = ps;
+                Ft = Fs;
+                if (cnt >= 2) {
+                    const uint32_t v = band[cnt - 2];
+                    ps = ln.pos(v);
+                    Fs = ln.height(v);
+                }
+            }
+            band[cnt++] = w;
+            ps = pt;
+            Fs = Ft;
+            pt = p;
+            Ft = F;
+        }
+        lo_i[b] = 0;
+        hi_i[b] = cnt;
+    }
+    __syncwarp();
+    // 2. merge neighbouring groups of s bands of the same line
+#pragma unroll
+    for (int s = 1; s < B; s <<= 1) {
+        if ((b & (2 * s - 1)) == 0) {
+            const int g = b, gm = g + s, ge = g + 2 * s;
+            int ta = gm - 1, tb = gm;
+            while (ta >= g && lo_i[ta] == hi_i[ta]) --ta;
+            while (tb < ge && lo_i[tb] == hi_i[tb]) ++tb;
+            if (ta >= g && tb < ge) {
+                int ia = hi_i[ta] - 1, ib = lo_i[tb];
+                uint32_t w = line[ta * (Lb + 1) + ia];
+                int pa = ln.pos(w), Fa = ln.height(w);
+                w = line[tb * (Lb + 1) + ib];
+                int pb = ln.pos(w), Fb = ln.height(w);
+                for (;;) {
+                    bool moved = false;
+                    // b moves right while its successor is on or below the line a-b
+                    for (;;) {
+                        int tn = tb, in_ = ib + 1;
+                        if (in_ >= hi_i[tn]) {
+                            ++tn;
+                            while (tn < ge && lo_i[tn] == hi_i[tn]) ++tn;
+                            if (tn >= ge) break;
+                            in_ = lo_i[tn];
+                        }
+                        const uint32_t wn = line[tn * (Lb + 1) + in_];
+                        const int pn = ln.pos(wn), Fn = ln.height(wn);
+                        if (below<WIDE>(pa, Fa, pb, Fb, pn, Fn)) break;
+                        tb = tn; ib = in_; pb = pn; Fb = Fn;
+                        moved = true;
+                    }
+                    // a moves left while it is on or above the segment from its predecessor to b
+                    for (;;) {
+                        int tp = ta, ip = ia - 1;
+                        if (ip < lo_i[tp]) {
+                            --tp;
+                            while (tp >= g && lo_i[tp] == hi_i[tp]) --tp;
+                            if (tp < g) break;
+                            ip = hi_i[tp] - 1;
+                        }
+                        const uint32_t wp = line[tp * (Lb + 1) + ip];
+                        const int pp = ln.pos(wp), Fp = ln.height(wp);
+                        if (below<WIDE>(pp, Fp, pa, Fa, pb, Fb)) break;
+                        ta = tp; ia = ip; pa = pp; Fa = Fp;
+                        moved = true;
+                    }
+                    if (!moved) break;
+                }
+                // cut both chains at the tangent
+                hi_i[ta] = ia + 1;
+                for (int t = ta + 1; t < gm; ++t) hi_i[t] = lo_i[t];
+                lo_i[tb] = ib;
+                for (int t = gm; t < tb; ++t) lo_i[t] = hi_i[t];
+            }
+        }
+        __syncwarp();
+    }
+    // 3. colour this lane's band from the hull, addressed by rank r through the
+    // surviving runs [lo, hi) of the line's bands
+    int P[B + 1];
+    P[0] = 0;
+#pragma unroll
+    for (int t = 0; t < B; ++t) P[t + 1] = P[t] + hi_i[t] - lo_i[t];
+    const int K = P[B];
+    auto word = [&](int r) {  // selects instead of an indexed array: P stays in registers
+        int t = 0, pt = 0;
+#pragma unroll
+        for (int u = 1; u < B; ++u)
+            if (r >= P[u]) { t = u; pt = P[u]; }
+        return line[t * (Lb + 1) + lo_i[t] + (r - pt)];
+    };
+    const int q0 = b * Lb;
+    if (K == 0) {
+        for (int j = 0; j < Lb; ++j) emit(i, q0 + j, MARKER);
+        return;
+    }
+    int kl = 0, kh = K - 1;  // the first hull point whose successor is not nearer to q0
+    while (kl < kh) {
+        const int m = (kl + kh) >> 1;
+        if (ln.dist(q0, word(m + 1)) >= ln.dist(q0, word(m))) kh = m;
+        else kl = m + 1;
+    }
+    // walk the hull over the band: point r is the nearest from q0 until the
+    // first position sw at which point r + 1 is at least as near,
+    //   (q - p1)^2 + f1 <= (q - p0)^2 + f0  <=>  2 q (p1 - p0) >= F1 - F0,
+    // so sw = ceil((F1 - F0) / (2 (p1 - p0))): a float quotient (both operands
+    // are exact in float) corrected by two integer tests
+    int r = kl;
+    uint32_t we = word(r);
+    int pe = ln.pos(we), Fe = ln.height(we);
+    auto next_switch = [&](int& sw, uint32_t& wn, int& pn, int& Fn) {
+        if (r + 1 >= K) {
+            sw = 1 << 30;
+            return;
+        }
+        wn = word(r + 1);
+        pn = ln.pos(wn);
+        Fn = ln.height(wn);
+        const int num = Fn - Fe, den = 2 * (pn - pe);
+        int t = (int)ceilf((float)num / (float)den);
+        if ((long long)t * den < num) ++t;
+        if ((long long)(t - 1) * den >= num) --t;
+        sw = t;
+    };
+    int sw;
+    uint32_t wn = 0;
+    int pn = 0, Fn = 0;
+    next_switch(sw, wn, pn, Fn);
+    const int q1 = q0 + Lb;
+    int q = q0;
+    while (q < q1) {
+        // the run of voxels nearest to point r inside this band
+        const int e = sw < q1 ? (sw > q ? sw : q) : q1;
+        for (; q < e; ++q) emit(i, q, we);
+        if (q >= q1) break;
+        ++r;
+        we = wn;
+        pe = pn;
+        Fe = Fn;
+        next_switch(sw, wn, pn, Fn);
+    }
+}
+
+// y pass output: site of voxel (x0 + i, q, z); with LPW = 8 the lanes of one
+// band store 8 consecutive words
+struct EmitY {
+    uint32_t* out;  // &out[z][0][x0]
+    int G;
+    __device__ __forceinline__ void operator()(int i, int q, uint32_t v) const { out[(size_t)q * G + i] = v; }
+};
+
+// x pass output: site of voxel (q, y0 + i, z), four consecutive sites per
+// 16-byte store (band starts are multiples of 4)
+struct EmitX {
+    uint32_t* out;  // &out[z][y0][0]
+    int G;
+    uint32_t v0, v1, v2;
+    __device__ __forceinline__ void operator()(int i, int q, uint32_t v) {
+        const int d = q & 3;
+        if (d == 0) v0 = v;
+        else if (d == 1) v1 = v;
+        else if (d == 2) v2 = v;
+        else *reinterpret_cast<uint4*>(out + (size_t)i * G + q - 3) = make_uint4(v0, v1, v2, v);
+    }
+};
+
+// Block (t, z, k): W warps, warp w stages lines l0 .. l0 + LPW - 1, l0 =
+// (t W + w) LPW, of plane z of grid k of the stack. AXIS 1: lines (x = l0 + i,
+// z) along y, rows of LPW words; AXIS 0: lines (y = l0 + i, z) along x, read as
+// 16-byte vectors.
+template <int AXIS, bool WIDE, int LPW, int W>
+__global__ void __launch_bounds__(32 * W) k_pba_env(int G, const uint32_t* __restrict__ in, uint32_t* __restrict__ out) {
+    G4D_DYN_SMEM(env_smem_raw);
+    constexpr int B = EnvTile<LPW>::B;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    EnvTile<LPW> T{G / B, G + B};
+    uint32_t* A = reinterpret_cast<uint32_t*>(env_smem_raw) + (size_t)warp * LPW * T.S;
+    int* lo = reinterpret_cast<int*>(reinterpret_cast<uint32_t*>(env_smem_raw) + (size_t)W * LPW * T.S) +
+              warp * 2 * LPW * B;
+    int* hi = lo + LPW * B;
+    const size_t plane = (size_t)G * G;
+    const size_t gbase = (size_t)blockIdx.z * plane * G + (size_t)blockIdx.y * plane;
+    const int l0 = (blockIdx.x * W + warp) * LPW;
+    // Staging: 16-byte chunks, a batch of 8 loads per lane in flight before
+    // any is stored. AXIS 1: chunk c holds 4 words of row y = c / (LPW / 4)
+    // (lines 4h .. 4h + 3, h = c % (LPW / 4)); AXIS 0: chunk c holds words
+    // 4c .. 4c + 3 of the tile's rows (line 4c / G, positions 4c % G ..).
+    constexpr int BATCH = 8;
+    const int nchunk = LPW * G / 4;
+    const uint4* src = AXIS ? reinterpret_cast<const uint4*>(in + gbase + l0)
+                            : reinterpret_cast<const uint4*>(in + gbase + (size_t)l0 * G);
+    for (int c0 = 0; c0 < nchunk; c0 += 32 * BATCH) {
+        uint4 v[BATCH];
+#pragma unroll
+        for (int k = 0; k < BATCH; ++k) {
+            const int c = c0 + k * 32 + lane;
+            if (c < nchunk) {
+                if constexpr (AXIS) v[k] = src[(size_t)(c / (LPW / 4)) * (G / 4) + c % (LPW / 4)];
+                else v[k] = src[c];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < BATCH; ++k) {
+            const int c = c0 + k * 32 + lane;
+            if (c >= nchunk) continue;
+            if constexpr (AXIS) {
+                const int y = c / (LPW / 4), h = c % (LPW / 4);
+                uint32_t* d = A + 4 * h * T.S + T.idx(y);
+                d[0] = v[k].x;
+                d[T.S] = v[k].y;
+                d[2 * T.S] = v[k].z;
+                d[3 * T.S] = v[k].w;
+            } else {
+                const int i = (c * 4) / G, x = (c * 4) % G;
+                uint32_t* d = A + i * T.S + T.idx(x);  // x .. x + 3 lie in one band
+                d[0] = v[k].x;
+                d[1] = v[k].y;
+                d[2] = v[k].z;
+                d[3] = v[k].w;
+            }
+        }
+    }
+    __syncwarp();
+    if (AXIS) {
+        EmitY em{out + gbase + l0, G};
+        env_lines<AXIS, WIDE, LPW>(G, T, A, lo, hi, l0, (int)blockIdx.y, em);
+    } else {
+        EmitX em{out + gbase + (size_t)l0 * G, G, 0, 0, 0};
+        env_lines<AXIS, WIDE, LPW>(G, T, A, lo, hi, l0, (int)blockIdx.y, em);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// The same passes with one thread per line (the other candidate of the
+// per-grid-width tuning in g4d_api.cu): no staging, the envelope's stack kept
+// as a list linked through the input words in global memory (the input is
+// scratch), full occupancy. On the 8M-point 1024^3 cloud this is the faster
+// form; at 512^3 and below the tiles are.
+//
+// Candidate p gives every voxel q of the line the squared distance
+// (q - p)^2 + f_p; the lower envelope is built in one downward sweep with a
+// stack whose links are written into the input word of each stacked candidate,
+// packed with the site coordinates the line does not fix, and read off in an
+// upward sweep at precomputed switch positions. Each thread keeps the two top
+// entries in registers, so a pop costs one load (of the new second).
+// ---------------------------------------------------------------------------
+constexpr uint32_t ENV_END = 2047;  // end of a list (11-bit link)
 
 // first position y at which candidate n (height fn) is at most as far as
 // candidate c (height fc), c < n: (n - c)(2y - n - c) >= fn - fc
@@ -186,7 +505,7 @@ struct EnvY {
 };
 
 template <bool WIDE>
-__global__ void __launch_bounds__(128) k_pba_env_y(int G, uint32_t* __restrict__ in, uint32_t* __restrict__ out) {
+__global__ void __launch_bounds__(128) k_pba_line_y(int G, uint32_t* __restrict__ in, uint32_t* __restrict__ out) {
     const int x = blockIdx.x * 32 + threadIdx.x;
     const int z = blockIdx.y * 4 + threadIdx.y;
     if (x >= G || z >= G) return;
@@ -256,7 +575,7 @@ struct EnvX {
 };
 
 template <bool WIDE>
-__global__ void __launch_bounds__(128) k_pba_env_x(int G, uint32_t* __restrict__ in, uint32_t* __restrict__ out) {
+__global__ void __launch_bounds__(128) k_pba_line_x(int G, uint32_t* __restrict__ in, uint32_t* __restrict__ out) {
     const int y = blockIdx.x * 32 + threadIdx.x;
     const int z = blockIdx.y * 4 + threadIdx.y;
     if (y >= G || z >= G) return;
@@ -469,21 +788,59 @@ void launch_pba_z_stack(const Launch& L, int G, int K, const unsigned long long*
     ++*L.launches;
 }
 
-void launch_pba_y(const Launch& L, int G, uint32_t* in, uint32_t* out) { launch_pba_y_stack(L, G, 1, in, out); }
-
-// `in` is scratch: the envelope passes keep their stacks in it
-void launch_pba_y_stack(const Launch& L, int G, int K, uint32_t* in, uint32_t* out) {
-    if (G > 512) k_pba_env_y<true><<<dim3(G / 32, G / 4, K), dim3(32, 4), 0, L.stream>>>(G, in, out);
-    else k_pba_env_y<false><<<dim3(G / 32, G / 4, K), dim3(32, 4), 0, L.stream>>>(G, in, out);
+template <int AXIS, int LPW, int W>
+static void launch_tiles(const Launch& L, int G, int K, const uint32_t* in, uint32_t* out) {
+    const size_t sm = W * env_warp_smem<LPW>(G);
+    const dim3 grid(G / (LPW * W), G, K), block(32 * W);
+    if (G > 512) {
+        cudaFuncSetAttribute(k_pba_env<AXIS, true, LPW, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_pba_env<AXIS, true, LPW, W><<<grid, block, sm, L.stream>>>(G, in, out);
+    } else {
+        cudaFuncSetAttribute(k_pba_env<AXIS, false, LPW, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k_pba_env<AXIS, false, LPW, W><<<grid, block, sm, L.stream>>>(G, in, out);
+    }
     ++*L.launches;
 }
 
-void launch_pba_x(const Launch& L, int G, uint32_t* in, uint32_t* out) { launch_pba_x_stack(L, G, 1, in, out); }
+int pba_default_form(int G) { return G >= 1024 ? PBA_LINES : PBA_TILES_4; }
 
-void launch_pba_x_stack(const Launch& L, int G, int K, uint32_t* in, uint32_t* out) {
-    if (G > 512) k_pba_env_x<true><<<dim3(G / 32, G / 4, K), dim3(32, 4), 0, L.stream>>>(G, in, out);
-    else k_pba_env_x<false><<<dim3(G / 32, G / 4, K), dim3(32, 4), 0, L.stream>>>(G, in, out);
-    ++*L.launches;
+bool pba_form_ok(int form, int G) { return form >= 0 && form < PBA_FORMS && (form != PBA_TILES_2 || G >= 64); }
+
+// `in` is scratch: the line form keeps its stacks in it
+void launch_pba_y_stack(const Launch& L, int G, int K, uint32_t* in, uint32_t* out, int form) {
+    if (!pba_form_ok(form, G)) form = pba_default_form(G);
+    if (form == PBA_LINES) {
+        const dim3 grid(G / 32, G / 4, K), block(32, 4);
+        if (G > 512) k_pba_line_y<true><<<grid, block, 0, L.stream>>>(G, in, out);
+        else k_pba_line_y<false><<<grid, block, 0, L.stream>>>(G, in, out);
+        ++*L.launches;
+    } else if (form == PBA_TILES_4) {
+        launch_tiles<1, 4, 4>(L, G, K, in, out);
+    } else {
+        launch_tiles<1, 4, 2>(L, G, K, in, out);
+    }
+}
+
+void launch_pba_x_stack(const Launch& L, int G, int K, uint32_t* in, uint32_t* out, int form) {
+    if (!pba_form_ok(form, G)) form = pba_default_form(G);
+    if (form == PBA_LINES) {
+        const dim3 grid(G / 32, G / 4, K), block(32, 4);
+        if (G > 512) k_pba_line_x<true><<<grid, block, 0, L.stream>>>(G, in, out);
+        else k_pba_line_x<false><<<grid, block, 0, L.stream>>>(G, in, out);
+        ++*L.launches;
+    } else if (form == PBA_TILES_4) {
+        launch_tiles<0, 4, 4>(L, G, K, in, out);
+    } else {
+        launch_tiles<0, 2, 2>(L, G, K, in, out);
+    }
+}
+
+void launch_pba_y(const Launch& L, int G, uint32_t* in, uint32_t* out, int form) {
+    launch_pba_y_stack(L, G, 1, in, out, form);
+}
+
+void launch_pba_x(const Launch& L, int G, uint32_t* in, uint32_t* out, int form) {
+    launch_pba_x_stack(L, G, 1, in, out, form);
 }
 
 // leader id at the voxel of every leader (the first point of its voxel in

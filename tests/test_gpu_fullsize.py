@@ -63,9 +63,11 @@ def _check(name, learned):
         with gstar4d_b200.Triangulator(grid_size=G, do_check=1) as t:
             nt, (dv, da), st = _device_digest(t, d_pts, len(pts))
     else:
-        # trained on another seeded cloud of the same configuration, as in the benchmark
-        train, _ = workloads.config_cloud(name, seed=1001)
-        with gstar4d_b200.Triangulator(grid_size=G) as tt:
+        # trained as in the benchmark: a 1/8-size cloud of the same
+        # configuration (another seed) at half the grid width, the same voxel
+        # density
+        train, _ = workloads.config_cloud(name, scale=1 / 8, seed=1001)
+        with gstar4d_b200.Triangulator(grid_size=G // 2) as tt:
             tt.train_proposal(train, epochs=2, lr=2e-3)
             w = tt.proposal_weights()
         with gstar4d_b200.Triangulator(grid_size=G, proposal=1, do_check=1) as t:

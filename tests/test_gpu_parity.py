@@ -179,3 +179,54 @@ def test_float32_points_match_the_widened_double_path(tri, oracle):
     ref, _, _ = oracle.triangulate(pts32.astype(np.float64), 256)
     r = oracle.canonical(ref)
     assert np.array_equal(ga[0], r[0]) and np.array_equal(ga[1], r[1])
+
+
+@pytest.mark.parametrize("name", ["mixed1m", "clustered8m"])
+def test_voronoi_exact_at_full_size_sampled(tri, oracle, name):
+    """The digital Voronoi diagram of the 1M (512^3) and 8M (1024^3)
+    configurations: on 2M sampled voxels the site is an occupied voxel at the
+    exact minimum squared distance (nearest occupied voxel by a k-d tree over
+    all of them; squared distances of integer points are compared as
+    integers)."""
+    from scipy.spatial import cKDTree
+    pts, G = workloads.config_cloud(name)
+    sites = tri.voronoi(pts, G)
+    _, vox = oracle.morton_order(pts, G)
+    occ = np.unique(vox.astype(np.int64), axis=0)
+    rng = np.random.default_rng(17)
+    idx = rng.integers(0, G ** 3, 2_000_000)
+    q = np.stack([idx % G, (idx // G) % G, idx // (G * G)], axis=1)
+    _, nn = cKDTree(occ).query(q)
+    d_ref = ((occ[nn] - q) ** 2).sum(axis=1)
+    s = sites[idx].astype(np.int64)
+    assert (s != 0xFFFFFFFF).all()
+    sv = np.stack([s & 1023, (s >> 10) & 1023, (s >> 20) & 1023], axis=1)
+    assert np.array_equal(((sv - q) ** 2).sum(axis=1), d_ref)
+    codes = set((occ[:, 0] | (occ[:, 1] << 10) | (occ[:, 2] << 20)).tolist())
+    assert all(int(c) in codes for c in np.unique(s))
+
+
+@pytest.mark.parametrize("form", [0, 1, 2])
+def test_every_pba_form_gives_the_same_triangulation(oracle, monkeypatch, form):
+    """The per-width tuner may pick any of the PBA pass forms (one thread per
+    line, or lines staged in shared memory in two tile shapes); each one gives
+    exact distances (test_voronoi_grid_is_exact covers the tuned one) and the
+    same triangulation."""
+    import gstar4d_b200
+    pts = workloads.clustered(40000, seed=23)
+    monkeypatch.setenv("G4D_PBA_FORM", str(form))
+    with gstar4d_b200.Triangulator(grid_size=128) as t:
+        sites = t.voronoi(pts, 128)
+        tets, _, _ = t.triangulate(pts)
+    _, vox = oracle.morton_order(pts, 128)
+    ref = oracle.edt(vox, 128)
+    g = np.arange(128)
+    Z, Y, X = np.meshgrid(g, g, g, indexing="ij")
+    s = sites.astype(np.int64)
+    d = (s & 1023) - X.ravel(), ((s >> 10) & 1023) - Y.ravel(), ((s >> 20) & 1023) - Z.ravel()
+    rv = vox[ref].astype(np.int64)
+    dr = rv[:, 0] - X.ravel(), rv[:, 1] - Y.ravel(), rv[:, 2] - Z.ravel()
+    assert np.array_equal(sum(c * c for c in d), sum(c * c for c in dr))
+    r, _, _ = oracle.triangulate(pts, 128)
+    a, b = _canon(oracle, tets), oracle.canonical(r)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
