@@ -63,12 +63,14 @@ WORKLOADS = {
 CPU_SAMPLE = {"clustered8m": 8, "mixed1m": 1, "degenerate500k": 1, "uniform100k": 1}
 REF_SAMPLE = {"clustered8m": 64, "mixed1m": 8, "degenerate500k": 8, "uniform100k": 1}
 
-# DRAM traffic of one PBA (z, y and x passes) per voxel, from ncu
-# (dram__bytes_read.sum + dram__bytes_write.sum of the three kernels, one
-# launch each, 512^3 grid); the capture and its command are in
-# profiles/pba_passes_mixed1m_g512.md. Scaled to a grid by its voxel count.
-PBA_TRAFFIC_PER_VOXEL = None
-PBA_TRAFFIC_SOURCE = "profiles/pba_passes_mixed1m_g512.md (ncu, 512^3)"
+# DRAM traffic of one PBA (z, y and x passes) per voxel for each form of the
+# y and x passes, from ncu (dram__bytes_read.sum + dram__bytes_write.sum of the
+# three kernels, one launch each) on a 1,000,000-point cloud of the clustered
+# configuration at 512^3 (the 8M cloud's voxel density); the capture and its
+# command are in profiles/pba_forms_clustered1m_g512.md. Scaled to a grid by
+# its voxel count (the passes' traffic is proportional to it).
+PBA_TRAFFIC_PER_VOXEL = {0: 4.929e9 / 512 ** 3, 1: 2.532e9 / 512 ** 3}
+PBA_TRAFFIC_SOURCE = "profiles/pba_forms_clustered1m_g512.md (ncu at 512^3, scaled by voxel count)"
 
 
 def _peaks():
@@ -501,7 +503,8 @@ def main():
         alg_bytes = 20.0 * G ** 3
         pba_avg = statistics.mean(pba_ms)
         achieved = alg_bytes / (pba_avg / 1e3) / 1e9
-        traffic = PBA_TRAFFIC_PER_VOXEL * G ** 3 if PBA_TRAFFIC_PER_VOXEL else None
+        form = last.get("pba_form", -1)
+        traffic = PBA_TRAFFIC_PER_VOXEL[form] * G ** 3 if form in PBA_TRAFFIC_PER_VOXEL else None
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "Mpts/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3), "higher_is_better": True,
@@ -510,7 +513,8 @@ def main():
                            l2="256 MB buffer written between timed steps", parallelism="replicas"),
             "e2e": {"value": round(e2e, 3), "unit": "Mpts/s", "h2d_bytes_per_step": int(n * 24),
                     "d2h_bytes_per_step": int(ntet_e2e * 32)},
-            "roofline": {"kernel": "pba (z, y, x passes)", "bound": "hbm", "achieved": round(achieved, 1),
+            "roofline": {"kernel": "pba (z, y, x passes; %s form)" % ("per-line" if form == 0 else "tile"),
+                         "bound": "hbm", "achieved": round(achieved, 1),
                          "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
                          "traffic": traffic, "traffic_source": PBA_TRAFFIC_SOURCE if traffic else None,
                          "algorithmic_bytes": alg_bytes, "avg_ms": round(pba_avg, 4)},

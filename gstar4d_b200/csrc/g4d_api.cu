@@ -659,6 +659,7 @@ g4d_status run_compute(g4d_ctx* ctx, bool map_to_input) {
     uint32_t* gA = ctx->b[B_GA].as<uint32_t>();
     uint32_t* gB = ctx->b[B_GB].as<uint32_t>();
     const int form = pba_form_for(ctx, D, gA, gB);
+    ctx->stats.pba_form = form;
     cudaEventRecord(ctx->ev[1], ctx->stream);
     // digital Voronoi diagram
     launch_pba_z(L, D, gA);

@@ -89,6 +89,8 @@ typedef struct {
     long long gpu_launches;      /* kernels launched by this call */
     int large_stars;             /* stars that outgrew the small storage class */
     int proposed;                /* candidate pairs the learned proposal added */
+    int pba_form;                /* form of the y and x passes used: 0 one thread per line,
+                                    1 and 2 lines staged in shared memory (tile shapes) */
 } g4d_stats;
 
 typedef struct g4d_ctx g4d_ctx;
