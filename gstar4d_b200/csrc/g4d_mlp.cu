@@ -147,16 +147,33 @@ __device__ void load_weight(unsigned char* dst, const float* W, int N, int K, bo
 // inference: logits of M candidate rows
 // ---------------------------------------------------------------------------
 
+// About 40 KB: layer 2's activations overwrite layer 1's in `a` (the MMA
+// that read them has completed), so four CTAs share an SM, each with 128
+// tensor-memory columns (z1 and z3 in columns 0..63, z2 in 64..127).
 struct InferSmem {
     unsigned char w1[64 * 16 * 2], w2[64 * 64 * 2], w3[64 * 64 * 2];
-    unsigned char x[128 * 16 * 2], a1[128 * 64 * 2], a2[128 * 64 * 2];
+    unsigned char x[128 * 16 * 2], a[128 * 64 * 2];
     float b[3 * 64 + 64 + 1];
     uint64_t bar;
     uint32_t tmem;
 };
 
+// relu(z + bias) of 16 accumulator columns, as BF16 (round to nearest even)
+// into columns c .. c + 15 of row t of a K-major A operand: two 16-byte stores
+__device__ __forceinline__ void store_act16(unsigned char* dst, int t, int c, const float* z, const float* bias) {
+    uint32_t pk[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const __nv_bfloat162 h =
+            __floats2bfloat162_rn(fmaxf(z[2 * i] + bias[2 * i], 0.f), fmaxf(z[2 * i + 1] + bias[2 * i + 1], 0.f));
+        pk[i] = *reinterpret_cast<const uint32_t*>(&h);
+    }
+    *reinterpret_cast<uint4*>(dst + kmaj(t, c, 128)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+    *reinterpret_cast<uint4*>(dst + kmaj(t, c + 8, 128)) = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+}
+
 // 128 threads; thread t owns row t of every tile (tensor-memory lane t)
-__global__ void __launch_bounds__(128, 1) k_mlp_infer(const float* __restrict__ P, const uint16_t* __restrict__ X,
+__global__ void __launch_bounds__(128, 4) k_mlp_infer(const float* __restrict__ P, const uint16_t* __restrict__ X,
                                                       int M, float* __restrict__ logits, unsigned* err) {
     extern __shared__ __align__(1024) unsigned char smem_raw_mlp[];
     InferSmem& S = *reinterpret_cast<InferSmem*>(smem_raw_mlp);
@@ -171,7 +188,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp_infer(const float* __restrict__ 
     }
     if (t == 0) mbar_init(&S.bar);
     if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 256;" ::"r"(smem_u32(&S.tmem)));
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 128;" ::"r"(smem_u32(&S.tmem)));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     tc_before_sync();
@@ -195,12 +212,12 @@ __global__ void __launch_bounds__(128, 1) k_mlp_infer(const float* __restrict__ 
         __syncthreads();
         tc_after_sync();
         float z[16];
-        unsigned char* aout[2] = {S.a1, S.a2};
         for (int layer = 0; layer < 3 && ok; ++layer) {
+            const uint32_t col = layer == 1 ? 64u : 0u;
             if (t == 0) {
-                const uint32_t a = smem_u32(layer == 0 ? S.x : (layer == 1 ? S.a1 : S.a2));
+                const uint32_t a = smem_u32(layer == 0 ? S.x : S.a);
                 const uint32_t b = smem_u32(layer == 0 ? S.w1 : (layer == 1 ? S.w2 : S.w3));
-                gemm(tb + 64u * layer, a, b, 64, layer == 0 ? 16 : 64, false);
+                gemm(tb + col, a, b, 64, layer == 0 ? 16 : 64, false);
                 umma_commit(&S.bar);
             }
             // a wait that ran out in any thread stops the whole block; the
@@ -214,12 +231,12 @@ __global__ void __launch_bounds__(128, 1) k_mlp_infer(const float* __restrict__ 
             tc_after_sync();
             float acc = 0.f;
             for (int c = 0; c < 64; c += 16) {
-                tmem_ld16(lane_addr + 64u * layer + c, z);
+                tmem_ld16(lane_addr + col + c, z);
+                if (layer < 2) {
+                    store_act16(S.a, t, c, z, S.b + 64 * layer + c);
+                } else {
 #pragma unroll
-                for (int i = 0; i < 16; ++i) {
-                    const float a = fmaxf(z[i] + S.b[64 * layer + c + i], 0.f);
-                    if (layer < 2) st_bf16(aout[layer], kmaj(t, c + i, 128), a);
-                    else acc = fmaf(a, S.b[192 + c + i], acc);
+                    for (int i = 0; i < 16; ++i) acc = fmaf(fmaxf(z[i] + S.b[128 + c + i], 0.f), S.b[192 + c + i], acc);
                 }
             }
             if (layer == 2 && row < M) logits[row] = acc + S.b[256];
@@ -235,7 +252,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp_infer(const float* __restrict__ 
     }
     tc_before_sync();
     __syncthreads();
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 256;" ::"r"(tb));
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 128;" ::"r"(tb));
 }
 
 // ---------------------------------------------------------------------------
@@ -547,8 +564,8 @@ void launch_mlp_infer(const Launch& L, const float* P, const uint16_t* X, int M,
     const int ntiles = (M + 127) / 128;
     const size_t sm = sizeof(InferSmem);
     cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    // two CTAs per SM: 256 tensor-memory columns each
-    int blocks = ntiles < 2 * 148 ? ntiles : 2 * 148;
+    // four CTAs per SM: 128 tensor-memory columns and about 40 KB of shared memory each
+    int blocks = ntiles < 4 * 148 ? ntiles : 4 * 148;
     k_mlp_infer<<<blocks < 1 ? 1 : blocks, 128, sm, L.stream>>>(P, X, M, logits, err);
     ++*L.launches;
 }

@@ -2,7 +2,13 @@
 //
 // For every point s the candidates are the distinct Voronoi sites within
 // Chebyshev distance 2 of s's voxel (a 5x5x5 block of the digital Voronoi grid),
-// each resolved to its point v (the voxel leader), v != s. Features of (s, v),
+// each resolved to its point v (the voxel leader), v != s, that is not already
+// in s's initial workset (the Voronoi pairs and missing-point pairs put there
+// before the proposal runs): the network only decides which further pairs to
+// add. Each unordered pair is scored once: from s when s < v, or from s when
+// s is not its voxel's leader (then s is no site, and v's block cannot name
+// it); a leader s > v is left to v's block, which names s because the
+// Chebyshev distance of their voxels is symmetric. Features of (s, v),
 // in grid units so that they do not depend on the cloud's extent:
 //   0..2  (v - s) / 2           offset
 //   3     |v - s| / 4           distance
@@ -26,6 +32,7 @@ __global__ void __launch_bounds__(128) k_ring(Dev D, Ring R) {
     __shared__ int hc[4][256];        // voxels per site
     __shared__ int list[4][128];      // occupied slots
     __shared__ int nlist[4];
+    __shared__ int wset[4][BUCKET_CAP];  // s's initial workset
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int G = R.cols.G;
     const int warps = gridDim.x * 4;
@@ -33,6 +40,9 @@ __global__ void __launch_bounds__(128) k_ring(Dev D, Ring R) {
         __syncwarp();
         for (int k = lane; k < 256; k += 32) { hs[w][k] = MARKER; hc[w][k] = 0; }
         if (lane == 0) nlist[w] = 0;
+        const int bc = min(D.bucketCount[s], BUCKET_CAP);
+        for (int k = lane; k < bc; k += 32) wset[w][k] = D.bucket[(size_t)s * BUCKET_CAP + k];
+        const bool leader = s == 0 || D.mkey[s - 1] != D.mkey[s];
         __syncwarp();
         const uint32_t e = D.vox[s];
         const int x = (int)vx(e), y = (int)vy(e), z = (int)vz(e);
@@ -62,7 +72,9 @@ __global__ void __launch_bounds__(128) k_ring(Dev D, Ring R) {
             if (j < nd) {
                 slot = list[w][j];
                 v = site_to_id(R.cols, hs[w][slot]);
-                if (v == s) v = -1;
+                if (v == s || (leader && v < s)) v = -1;
+                for (int k = 0; k < bc && v >= 0; ++k)
+                    if (wset[w][k] == v) v = -1;
             }
             const unsigned m = __ballot_sync(0xffffffffu, v >= 0);
             int cnt = __popc(m);
