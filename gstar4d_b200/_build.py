@@ -17,7 +17,7 @@ LIB = os.path.join(HERE, "libgstar4d.so")
 EXE = os.path.join(HERE, "gstar4d")  # native command line
 OBJ = os.path.join(HERE, "_build")
 
-SOURCES = ["g4d_order.cu", "g4d_pba.cu", "g4d_star.cu", "g4d_api.cu", "g4d_noalloc.cu", "g4d_mlp.cu", "g4d_proposal.cu", "g4d_check.cu", "g4d_points.cpp"]
+SOURCES = ["g4d_order.cu", "g4d_pba.cu", "g4d_star.cu", "g4d_api.cu", "g4d_noalloc.cu", "g4d_mlp.cu", "g4d_proposal.cu", "g4d_block.cu", "g4d_check.cu", "g4d_points.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
          "-I", os.path.join(REPO, "include"), "-I", CSRC, "--expt-relaxed-constexpr"]

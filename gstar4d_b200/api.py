@@ -56,7 +56,8 @@ class Stats(ctypes.Structure):
                 ("drowned", ctypes.c_longlong), ("proofs", ctypes.c_longlong),
                 ("exact_predicates", ctypes.c_longlong), ("loops", ctypes.c_int), ("missing", ctypes.c_int),
                 ("grid_size", ctypes.c_int), ("tets", ctypes.c_int), ("gpu_launches", ctypes.c_longlong),
-                ("large_stars", ctypes.c_int), ("proposed", ctypes.c_int), ("pba_form", ctypes.c_int)]
+                ("large_stars", ctypes.c_int), ("proposed", ctypes.c_int), ("pba_form", ctypes.c_int),
+                ("block_pairs", ctypes.c_int)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

@@ -102,6 +102,7 @@ struct g4d_ctx {
     std::map<int, int> tuned;  // autotuner: (size bucket, distribution class) -> grid width
     std::map<int, int> pba_form;  // autotuner: grid width -> fastest PBA pass form
     int next_grid = 0;         // tuned width for the next single-cloud call (0: none)
+    int block_k = BLOCK_K_DEFAULT;  // voxel-block workset pairs per point (0: none)
     // learned star proposal
     bool has_model = false;
     int adam_step = 0;
@@ -339,6 +340,11 @@ g4d_status alloc_stars(g4d_ctx* ctx, int n) {
     return G4D_OK;
 }
 
+// Entries both drowned lists hold (their byte sizes may pass 2 GiB).
+int drown_cap(const g4d_ctx* ctx) {
+    return (int)std::min<size_t>(std::min(ctx->b[B_DROWN].cap, ctx->b[B_DROWN2].cap) / sizeof(int2), 0x7fffffff);
+}
+
 // Grow both overflow request lists to hold `need` entries, keeping the
 // current list's first `keep` entries.
 g4d_status grow_ovf(g4d_ctx* ctx, Dev& D, int keep, size_t need) {
@@ -364,12 +370,24 @@ g4d_status worksets_fit(g4d_ctx* ctx, Dev& D, int attempt, bool* again) {
     CK(cudaMemcpyAsync(&h, D.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, ctx->stream));
     CK_SYNC(ctx->stream);
     *again = false;
-    if (h.ovf_next <= D.ovfCap) return G4D_OK;
+    if (h.ovf_next <= D.ovfCap) {
+        // every candidate the initial build inserts may drown: room for all
+        const size_t need = std::min<size_t>(std::max<size_t>(16 * (size_t)D.n, h.cand_total + 1024), 0x7fffffff);
+        if (need > (size_t)D.drownCap) {
+            CK(ctx->b[B_DROWN].ensure(sizeof(int2) * need));
+            CK(ctx->b[B_DROWN2].ensure(sizeof(int2) * need));
+            D.drown = ctx->b[B_DROWN].as<int2>();
+            D.drownNext = ctx->b[B_DROWN2].as<int2>();
+            D.drownCap = drown_cap(ctx);
+        }
+        return G4D_OK;
+    }
     if (attempt >= 2) return fail(ctx, G4D_ERR_CAPACITY, "overflow request list capacity exceeded");
     g4d_status st = grow_ovf(ctx, D, 0, 2 * (size_t)h.ovf_next + (size_t)D.n);
     if (st) return st;
     CK(cudaMemsetAsync(&D.ctr->ovf_next, 0, sizeof(int), ctx->stream));
     CK(cudaMemsetAsync(&D.ctr->proposed, 0, sizeof(int), ctx->stream));
+    CK(cudaMemsetAsync(&D.ctr->block_pairs, 0, sizeof(int), ctx->stream));
     h.err &= ~(unsigned)ERR_OVFCAP;
     CK(cudaMemcpyAsync(&D.ctr->err, &h.err, sizeof(unsigned), cudaMemcpyHostToDevice, ctx->stream));
     CK_SYNC(ctx->stream);
@@ -490,6 +508,7 @@ g4d_status run_splay(g4d_ctx* ctx, Dev& D) {
     ctx->stats.proofs = (long long)h.proofs_total;
     ctx->stats.exact_predicates = (long long)h.exact;
     ctx->stats.proposed = h.proposed;
+    ctx->stats.block_pairs = h.block_pairs;
     ctx->large_used = h.large_next;
 
     if (ctx->cfg.do_check) {
@@ -654,7 +673,7 @@ g4d_status run_compute(g4d_ctx* ctx, bool map_to_input) {
     if (st) return st;
     Dev D = make_dev(ctx);
     // equalise the two drowned buffers' capacity
-    D.drownCap = (int)std::min(ctx->b[B_DROWN].cap, ctx->b[B_DROWN2].cap) / (int)sizeof(int2);
+    D.drownCap = drown_cap(ctx);
 
     uint32_t* gA = ctx->b[B_GA].as<uint32_t>();
     uint32_t* gB = ctx->b[B_GB].as<uint32_t>();
@@ -673,8 +692,10 @@ g4d_status run_compute(g4d_ctx* ctx, bool map_to_input) {
         launch_site_map(L, D, reinterpret_cast<int*>(gB));
         launch_pairs(L, D, gA, reinterpret_cast<int*>(gB));
         launch_missing(L, D);
+        if (ctx->block_k > 0) launch_block_pairs(L, D, gA, reinterpret_cast<const int*>(gB), ctx->block_k);
         st = run_proposal(ctx, D);
         if (st) return st;
+        launch_workset_total(L, D);
         bool again = false;
         st = worksets_fit(ctx, D, attempt, &again);
         if (st) return st;
@@ -878,7 +899,7 @@ g4d_status run_wave(g4d_ctx* ctx, const double* d_xyz, const int64_t* offs, cons
     launch_colranges_u64(L, ckey, n, cs, ce);
 
     Dev D = make_dev(ctx);
-    D.drownCap = (int)std::min(ctx->b[B_DROWN].cap, ctx->b[B_DROWN2].cap) / (int)sizeof(int2);
+    D.drownCap = drown_cap(ctx);
     D.G = 0;
     D.cloudOff = d_slotW;
     D.nclouds = ns;
@@ -1225,6 +1246,7 @@ g4d_status g4d_create(g4d_ctx** out, const g4d_config* cfg) {
         for (int G = 32; G <= 1024; G *= 2)
             if (pba_form_ok(form, G)) ctx->pba_form[G] = form;
     }
+    if (const char* f = std::getenv("G4D_BLOCK_K")) ctx->block_k = std::max(0, std::min(std::atoi(f), 64));
     if (const char* f = std::getenv("G4D_FAIL_ALLOC_AFTER")) {
         ctx->budget.left = std::atoll(f);
         for (auto& b : ctx->b) b.budget = &ctx->budget;

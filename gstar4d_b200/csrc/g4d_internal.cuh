@@ -51,6 +51,7 @@ constexpr int LTSTRIDE = 2048;            // large: triangle slots in HBM
 constexpr int BUCKET_CAP = 64;            // initial candidates kept per star
 constexpr int INBOX_CAP = 64;             // insertion requests per star per round
 constexpr int MIN_WORKSET = 8;            // GDelCommon.h:49
+constexpr int BLOCK_K_DEFAULT = 16;       // voxel-block workset pairs per point
 constexpr uint32_t HEMPTY = 0x7fffffffu;
 constexpr uint32_t HLINK = 0x80000000u;
 constexpr uint32_t HID = 0x7fffffffu;
@@ -97,6 +98,8 @@ struct Counters {
     double dbg_pts[15];
     int dbg_ids[5];
     int fix_next;         // tetra output: neighbour links written by the other side
+    int block_pairs;      // workset pairs added from voxel blocks
+    unsigned long long cand_total;  // initial star insertions at most (sum over the worksets)
 };
 
 __host__ __device__ inline uint32_t enc_vox(uint32_t x, uint32_t y, uint32_t z) { return x | (y << 10) | (z << 20); }
@@ -266,6 +269,12 @@ void launch_pba_x_stack(const Launch& L, int G, int K, uint32_t* in, uint32_t* o
 void launch_pairs_stack(const Launch& L, const Dev& D, const uint32_t* stack, int* map, int G, int K,
                         const unsigned long long* ckey, const int* cid, const int* cs, const int* ce);
 void launch_missing_u64(const Launch& L, const Dev& D, const unsigned long long* mkey);
+// workset pairs of each point with its k_sel nearest points of the 3x3x3 voxel
+// block (single clouds; the insertion-request arrays serve as scratch)
+void launch_block_pairs(const Launch& L, const Dev& D, const uint32_t* grid, const int* map, int k_sel);
+// ctr->cand_total = sum over stars of the initial insertions they can make
+// (the workset, pumped up to MIN_WORKSET): the initial build's drowned points
+void launch_workset_total(const Launch& L, const Dev& D);
 
 // stars
 // Star kernels run first filter-only (exact = false: FP64 filter, no exact

@@ -91,6 +91,7 @@ typedef struct {
     int proposed;                /* candidate pairs the learned proposal added */
     int pba_form;                /* form of the y and x passes used: 0 one thread per line,
                                     1 and 2 lines staged in shared memory (tile shapes) */
+    int block_pairs;             /* workset pairs added from 3x3x3 voxel blocks */
 } g4d_stats;
 
 typedef struct g4d_ctx g4d_ctx;

@@ -101,6 +101,43 @@ def test_parity_dense_voxels_overflow_worksets(oracle):
     assert np.array_equal(g[1], r[1]), "adjacency differs"
 
 
+def _clustered_dense(k):
+    import gstar4d_b200
+    pts = workloads.clustered(120000, k=16, sigma=0.01, seed=12)
+    os.environ["G4D_BLOCK_K"] = str(k)
+    try:
+        with gstar4d_b200.Triangulator(grid_size=128, do_check=1) as t:
+            tets, _, st = t.triangulate(pts)
+    finally:
+        del os.environ["G4D_BLOCK_K"]
+    return pts, tets, st
+
+
+@pytest.mark.parametrize("k", [1, 64])
+def test_block_pairs_leave_the_triangulation_unchanged(oracle, k):
+    """Workset pairs from 3x3x3 voxel blocks (the G4D_BLOCK_K nearest block
+    points of every point whose voxel holds several points) only change
+    splaying's work: a clustered cloud with several points in many voxels
+    triangulates as the oracle does for any K."""
+    pts, tets, st = _clustered_dense(k)
+    ref, _, _ = oracle.triangulate(pts, 128)
+    g, r = _canon(oracle, tets), oracle.canonical(ref)
+    assert np.array_equal(g[0], r[0]), "tetrahedra differ"
+    assert np.array_equal(g[1], r[1]), "adjacency differs"
+    assert st["block_pairs"] > 0
+
+
+def test_block_pairs_save_splaying_work(oracle):
+    """The default K against none: the same triangulation, fewer insertions
+    left to splaying."""
+    pts, tets0, st0 = _clustered_dense(0)
+    _, tets, st = _clustered_dense(16)
+    assert st0["block_pairs"] == 0 and st["block_pairs"] > 0
+    a, b = _canon(oracle, tets0), _canon(oracle, tets)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+    assert st["splay_insertions"] < 0.8 * st0["splay_insertions"]
+
+
 def test_morton_index_space_and_gdel_entry_points(oracle):
     """gdelInit/gdelCompute/getTetraFromGpu shape: points already in grid units,
     overwritten with the Morton order; output in Morton indices."""
