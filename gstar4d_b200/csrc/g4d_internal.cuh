@@ -201,8 +201,8 @@ __device__ __forceinline__ int site_to_id(const Cols<KeyT>& C, uint32_t e) {
 // Initial workset entry b of point a. Worksets are symmetric (b in a's <=> a in
 // b's), which splaying relies on; an entry that finds a's workset full becomes
 // an insertion request sent after the initial stars are built.
-__device__ __forceinline__ void bucket_push(const Dev& D, int a, int b) {
-    const int pos = atomicAdd(&D.bucketCount[a], 1);
+// entry b of a's workset at position pos (taken from bucketCount[a])
+__device__ __forceinline__ void bucket_put(const Dev& D, int a, int b, int pos) {
     if (pos < BUCKET_CAP) {
         D.bucket[(size_t)a * BUCKET_CAP + pos] = b;
         return;
@@ -210,6 +210,9 @@ __device__ __forceinline__ void bucket_push(const Dev& D, int a, int b) {
     const int q = atomicAdd(&D.ctr->ovf_next, 1);
     if (q < D.ovfCap) D.ovfNext[q] = make_int2(a, b);
     else atomicOr(&D.ctr->err, ERR_OVFCAP);
+}
+__device__ __forceinline__ void bucket_push(const Dev& D, int a, int b) {
+    bucket_put(D, a, b, atomicAdd(&D.bucketCount[a], 1));
 }
 
 // ---- launchers (host) --------------------------------------------------------

@@ -602,7 +602,15 @@ __global__ void __launch_bounds__(128) k_pba_line_x(int G, uint32_t* __restrict_
 #define PAIR_WARPS_DEF 4
 #endif
 constexpr int PAIR_HASH = 1 << PAIR_HASH_LOG2;  // block hash entries (8 bytes each)
-constexpr int PAIR_PROBES = 32;
+// probes of a pair insert before it goes to the worksets directly: inside
+// dense clusters nearly every cube holds eight sites and the block's pairs
+// outnumber the table, where a long probe walk costs more than the duplicate
+// pushes it saves
+#ifndef PAIR_PROBES_DEF
+#define PAIR_PROBES_DEF 4
+#endif
+constexpr int PAIR_PROBES = PAIR_PROBES_DEF;
+constexpr int PAIR_BATCH = 4;  // hash entries per thread in flight in the final scatter
 constexpr int PAIR_ZC = PAIR_ZC_DEF;            // cube planes per block
 constexpr int PAIR_WARPS = PAIR_WARPS_DEF;      // warps per block, one row of x each
 
@@ -627,44 +635,85 @@ __device__ __forceinline__ void pair_hash_insert(unsigned long long* hs, unsigne
 // around digital Voronoi vertices, GDelKernels.cu:137-299). One thread sweeps a
 // column of cubes along z, keeping the previous voxel plane in registers and
 // loading the plane after the next one ahead of use (4 loads per cube,
-// coalesced over x). The distinct sites of a cube are a bit mask computed
-// without branches (bit i: voxel i differs from voxels 0..i-1), so every lane
-// does the same few dozen instructions per cube. Vertex cubes are rare (about
-// 5% of the cubes): a lane queues the site set of each one (skipping a repeat
-// of its previous set) in a per-warp queue, and every 32 queued cubes the warp
-// emits their pairs, one cube per lane, into a block-local hash that removes
-// duplicates before the per-star scatter.
-// all pairs of one queued vertex cube into the block hash
-template <class KeyT>
-__device__ __forceinline__ void emit_cube(unsigned long long* hs, const uint32_t* q, int ns, const Dev& D,
-                                          const Cols<KeyT>& C) {
-    for (int i = 0; i < ns; ++i)
-        for (int j = i + 1; j < ns; ++j) {
-            const uint32_t lo = q[i] < q[j] ? q[i] : q[j], hi = q[i] < q[j] ? q[j] : q[i];
-            pair_hash_insert(hs, ((unsigned long long)lo << 32) | hi, D, C);
-        }
+// coalesced over x). Each 2x2 face gets its distinct-site count and its
+// smallest and largest site once (the two cubes that share it reuse them).
+// A cube holds fewer than four sites when its faces' counts add up to less
+// than four, or when both faces hold the same two sites (a cube on a Voronoi
+// wall, the common case away from clusters). The cubes left (near Voronoi
+// edges and vertices, and inside dense clusters) go to a per-warp queue;
+// every 32 queued cubes the warp takes one per lane, computes its distinct
+// sites and emits the pairs of the vertex cubes, spread over the lanes, into a
+// block-local hash that removes duplicates before the per-star scatter.
+constexpr int PAIR_QUEUE = 64;  // queued cubes per warp
+
+struct Face {
+    int n;           // distinct sites
+    uint32_t lo, hi;  // smallest and largest site
+};
+
+__device__ __forceinline__ Face face_of(uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+    Face f;
+    f.n = 1 + (b != a) + (c != a && c != b) + (d != a && d != b && d != c);
+    f.lo = min(min(a, b), min(c, d));
+    f.hi = max(max(a, b), max(c, d));
+    return f;
 }
 
-constexpr int PAIR_QUEUE = 64;  // queued vertex cubes per warp
-
-// bit i set when v[i] differs from v[0..i-1]; v[0..3] is the lower plane
-__device__ __forceinline__ uint32_t distinct_mask(const uint32_t (&v)[8]) {
-    uint32_t m = 1u;
+// The 32 queued cubes qs[0..32) of a warp, one per lane: each lane reduces its
+// cube to its distinct sites (in place); the pairs of the vertex cubes (four
+// or more sites: n(n-1)/2 pairs, up to 28) are then spread over the lanes, 32
+// at a time, so that a cube of eight sites does not hold up the warp. Pair k
+// of a cube is (i, j) in colexicographic order: j(j-1)/2 <= k < j(j+1)/2,
+// i = k - j(j-1)/2.
+template <class KeyT>
+__device__ __forceinline__ void emit_queued(unsigned long long* hs, uint32_t (*qs)[8], int* qoff, int lane, int nq,
+                                            const Dev& D, const Cols<KeyT>& C) {
+    int np = 0;
+    if (lane < nq) {
+        uint32_t* q = qs[lane];
+        uint32_t v[8];
 #pragma unroll
-    for (int i = 1; i < 8; ++i) {
-        bool fresh = true;
+        for (int k = 0; k < 8; ++k) v[k] = q[k];
+        int ns = 0;
 #pragma unroll
-        for (int j = 0; j < i; ++j) fresh = fresh && (v[i] != v[j]);
-        m |= (uint32_t)fresh << i;
+        for (int i = 0; i < 8; ++i) {
+            bool fresh = true;
+#pragma unroll
+            for (int j = 0; j < i; ++j) fresh = fresh && (v[i] != v[j]);
+            if (fresh) q[ns++] = v[i];
+        }
+        np = ns >= 4 ? ns * (ns - 1) / 2 : 0;
     }
-    return m;
+    int incl = np;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl += t;
+    }
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    qoff[lane] = incl - np;
+    __syncwarp();
+    for (int p = lane; p < total; p += 32) {
+        // the last cube whose first pair is at or before p (it has pairs)
+        int c = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1)
+            if (qoff[c + step] <= p) c += step;
+        const int k = p - qoff[c];
+        int j = 1;
+        while ((j + 1) * j / 2 <= k) ++j;
+        const int i = k - j * (j - 1) / 2;
+        const uint32_t a = qs[c][i], b = qs[c][j];
+        pair_hash_insert(hs, a < b ? ((unsigned long long)a << 32) | b : ((unsigned long long)b << 32) | a, D, C);
+    }
+    __syncwarp();
 }
 
 template <class KeyT>
 __global__ void __launch_bounds__(32 * PAIR_WARPS) k_pairs(Dev D, const uint32_t* __restrict__ stack, Cols<KeyT> C, int nzc) {
     __shared__ unsigned long long hs[PAIR_HASH];
-    __shared__ uint32_t qs[PAIR_WARPS][PAIR_QUEUE][8];  // site sets of vertex cubes
-    __shared__ uint8_t qn[PAIR_WARPS][PAIR_QUEUE];
+    __shared__ uint32_t qs[PAIR_WARPS][PAIR_QUEUE][8];  // voxel sites of queued cubes
+    __shared__ int qoff[PAIR_WARPS][32];                // first pair of each of 32 queued cubes
     const int G = C.G;
     const int tid = threadIdx.y * 32 + threadIdx.x;
     for (int k = tid; k < PAIR_HASH; k += 32 * PAIR_WARPS) hs[k] = ~0ull;
@@ -680,16 +729,16 @@ __global__ void __launch_bounds__(32 * PAIR_WARPS) k_pairs(Dev D, const uint32_t
     if (C.map) C.map += (size_t)kk * plane * G;
     const int lane = threadIdx.x, w = threadIdx.y;
     // every lane of the warp walks the same z range so the warp collectives
-    // below stay converged; lanes past the grid edge carry no pairs (they read
+    // below stay converged; lanes past the grid edge queue nothing (they read
     // column 0, which is in bounds)
     const bool active = x < G - 1 && y < G - 1;
     const int zend = min(z0 + PAIR_ZC, G - 1);
     if (y < G - 1 && z0 < G - 1) {
         const uint32_t* g = grid + (size_t)y * G + (active ? x : 0);
-        uint32_t v[8];
+        uint32_t v0, v1, v2, v3;
         {
             const size_t o = (size_t)z0 * plane;
-            v[0] = g[o]; v[1] = g[o + 1]; v[2] = g[o + G]; v[3] = g[o + G + 1];
+            v0 = g[o]; v1 = g[o + 1]; v2 = g[o + G]; v3 = g[o + G + 1];
         }
         // plane z0+1 exists: z0 < G-1
         uint32_t n0, n1, n2, n3;
@@ -697,66 +746,67 @@ __global__ void __launch_bounds__(32 * PAIR_WARPS) k_pairs(Dev D, const uint32_t
             const size_t o = (size_t)(z0 + 1) * plane;
             n0 = g[o]; n1 = g[o + 1]; n2 = g[o + G]; n3 = g[o + G + 1];
         }
-        unsigned long long last = 0;  // signature of the set this lane queued last
-        int qc = 0;                   // queued cubes of this warp (same in every lane)
+        Face fl = face_of(v0, v1, v2, v3);
+        int qc = 0;  // queued cubes of this warp (same in every lane)
         for (int z = z0; z < zend; ++z) {
-            v[4] = n0; v[5] = n1; v[6] = n2; v[7] = n3;
+            const uint32_t u0 = n0, u1 = n1, u2 = n2, u3 = n3;
             if (z + 1 < zend) {  // the plane after the next one, loaded ahead of use
                 const size_t o = (size_t)(z + 2) * plane;
                 n0 = g[o]; n1 = g[o + 1]; n2 = g[o + G]; n3 = g[o + G + 1];
             }
-            bool cand = false;
-            uint32_t m = 0;
-            // a warp whose cubes all lie inside one Voronoi cell each skips the mask
-            const bool mixed = (v[1] != v[0]) | (v[2] != v[0]) | (v[3] != v[0]) | (v[4] != v[0]) |
-                               (v[5] != v[0]) | (v[6] != v[0]) | (v[7] != v[0]);
-            if (__any_sync(0xffffffffu, active && mixed)) {
-                m = distinct_mask(v);
-                if (active && __popc(m) >= 4) {
-                    // consecutive cubes around one Voronoi vertex repeat its set
-                    unsigned long long sum = 0, xr = 0;
+            const Face fu = face_of(u0, u1, u2, u3);
+            const bool wall = fl.n == 2 && fu.n == 2 && fl.lo == fu.lo && fl.hi == fu.hi;
+            const bool maybe = active && fl.n + fu.n >= 4 && !wall;
+            const unsigned bal = __ballot_sync(0xffffffffu, maybe);
+            if (bal) {
+                if (maybe) {
+                    uint32_t* q = qs[w][qc + __popc(bal & ((1u << lane) - 1u))];
+                    q[0] = v0; q[1] = v1; q[2] = v2; q[3] = v3;
+                    q[4] = u0; q[5] = u1; q[6] = u2; q[7] = u3;
+                }
+                qc += __popc(bal);
+                if (qc >= 32) {  // one queued cube per lane
+                    __syncwarp();
+                    emit_queued(hs, qs[w], qoff[w], lane, 32, D, C);
+                    for (int k = 32 + lane; k < qc; k += 32)
 #pragma unroll
-                    for (int k = 0; k < 8; ++k)
-                        if (m >> k & 1u) { sum += v[k]; xr ^= (unsigned long long)v[k] * 0x9E3779B97F4A7C15ull; }
-                    const unsigned long long sig = (sum << 32) ^ xr ^ (unsigned long long)__popc(m);
-                    cand = sig != last;
-                    last = sig;
+                        for (int i = 0; i < 8; ++i) qs[w][k - 32][i] = qs[w][k][i];
+                    qc -= 32;
+                    __syncwarp();
                 }
             }
-            const unsigned bal = __ballot_sync(0xffffffffu, cand);
-            if (cand) {
-                const int pos = qc + __popc(bal & ((1u << lane) - 1u));
-                int ns = 0;
-#pragma unroll
-                for (int k = 0; k < 8; ++k)
-                    if (m >> k & 1u) qs[w][pos][ns++] = v[k];
-                qn[w][pos] = (uint8_t)ns;
-            }
-            qc += __popc(bal);
-            if (qc >= 32) {  // one queued cube per lane
-                __syncwarp();
-                emit_cube(hs, qs[w][lane], qn[w][lane], D, C);
-                __syncwarp();
-                for (int k = 32 + lane; k < qc; k += 32) {
-                    for (int q = 0; q < qn[w][k]; ++q) qs[w][k - 32][q] = qs[w][k][q];
-                    qn[w][k - 32] = qn[w][k];
-                }
-                qc -= 32;
-                __syncwarp();
-            }
-            v[0] = v[4]; v[1] = v[5]; v[2] = v[6]; v[3] = v[7];
+            v0 = u0; v1 = u1; v2 = u2; v3 = u3;
+            fl = fu;
         }
         __syncwarp();
-        if (lane < qc) emit_cube(hs, qs[w][lane], qn[w][lane], D, C);
+        emit_queued(hs, qs[w], qoff[w], lane, qc, D, C);
     }
     __syncthreads();
-    for (int k = tid; k < PAIR_HASH; k += 32 * PAIR_WARPS) {
-        const unsigned long long key = hs[k];
-        if (key == ~0ull) continue;
-        const int ia = site_to_id(C, (uint32_t)(key >> 32)), ib = site_to_id(C, (uint32_t)key);
-        if (ia >= 0 && ib >= 0) {
-            bucket_push(D, ia, ib);
-            bucket_push(D, ib, ia);
+    // the block's distinct pairs to both stars' worksets, PAIR_BATCH entries per
+    // thread at a time so that their map loads and workset atomics overlap
+    for (int k0 = tid; k0 < PAIR_HASH; k0 += PAIR_BATCH * 32 * PAIR_WARPS) {
+        int ia[PAIR_BATCH], ib[PAIR_BATCH];
+#pragma unroll
+        for (int j = 0; j < PAIR_BATCH; ++j) {
+            const int k = k0 + j * 32 * PAIR_WARPS;
+            const unsigned long long key = k < PAIR_HASH ? hs[k] : ~0ull;
+            ia[j] = ib[j] = -1;
+            if (key != ~0ull) {
+                ia[j] = site_to_id(C, (uint32_t)(key >> 32));
+                ib[j] = site_to_id(C, (uint32_t)key);
+            }
+        }
+        int pa[PAIR_BATCH], pb[PAIR_BATCH];
+#pragma unroll
+        for (int j = 0; j < PAIR_BATCH; ++j) {
+            const bool ok = ia[j] >= 0 && ib[j] >= 0;
+            pa[j] = ok ? atomicAdd(&D.bucketCount[ia[j]], 1) : -1;
+            pb[j] = ok ? atomicAdd(&D.bucketCount[ib[j]], 1) : -1;
+        }
+#pragma unroll
+        for (int j = 0; j < PAIR_BATCH; ++j) {
+            if (pa[j] >= 0) bucket_put(D, ia[j], ib[j], pa[j]);
+            if (pb[j] >= 0) bucket_put(D, ib[j], ia[j], pb[j]);
         }
     }
 }

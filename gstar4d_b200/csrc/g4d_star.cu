@@ -876,6 +876,42 @@ __global__ void __launch_bounds__(32 * C::WARPS, EXACT ? C::MINB : C::MINB_FAST)
                 }
             __syncwarp();
             if (lane < nins) S.order[lane] = (typename C::Slot)slot;
+        } else if (nins <= 64) {
+            // two candidates per lane (element lane + 32 r in register r): the
+            // same network over 64 elements; j = 32 compares a lane's own pair
+            float key[2];
+            int slot[2];
+#pragma unroll
+            for (int r = 0; r < 2; ++r) {
+                const int i = lane + 32 * r;
+                key[r] = i < nins ? S.okey[i] : 3.0e38f;
+                slot[r] = i < nins ? (int)S.order[i] : 0x7fffffff;
+            }
+#pragma unroll
+            for (int k = 2; k <= 64; k <<= 1)
+#pragma unroll
+                for (int j = k >> 1; j > 0; j >>= 1) {
+                    if (j == 32) {  // k = 64: ascending, register 0 keeps the smaller
+                        if (key[1] < key[0] || (key[1] == key[0] && slot[1] < slot[0])) {
+                            const float tk = key[0]; key[0] = key[1]; key[1] = tk;
+                            const int ts = slot[0]; slot[0] = slot[1]; slot[1] = ts;
+                        }
+                        continue;
+                    }
+#pragma unroll
+                    for (int r = 0; r < 2; ++r) {
+                        const float ok = __shfl_xor_sync(0xffffffffu, key[r], j);
+                        const int os = __shfl_xor_sync(0xffffffffu, slot[r], j);
+                        const bool other_less = ok < key[r] || (ok == key[r] && os < slot[r]);
+                        const int i = lane + 32 * r;
+                        const bool keep_small = ((lane & j) == 0) == ((i & k) == 0);
+                        if (keep_small == other_less) { key[r] = ok; slot[r] = os; }
+                    }
+                }
+            __syncwarp();
+#pragma unroll
+            for (int r = 0; r < 2; ++r)
+                if (lane + 32 * r < nins) S.order[lane + 32 * r] = (typename C::Slot)slot[r];
         } else {
             warp_sort_order(S, lane, nins);
         }
