@@ -1201,14 +1201,28 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK, EXACT ? 4 : PROOF_BLOCKS
         from_list = queued <= D.n;
         if (from_list) count = queued;
     }
-    for (int w = blockIdx.x * WARPS_PER_BLOCK + (threadIdx.x >> 5); w < count; w += warps) {
+    // A proof is needed only while v's star still links back to s, which most
+    // drowned points' stars no longer do: the filter-only kernel takes 32 items
+    // per warp at a time, every lane checks one, and the warp then searches the
+    // proofs of those left. The exact kernel's items (the few the filter could
+    // not decide, each costly) go one per warp.
+    constexpr int PER = EXACT ? 1 : 32;
+    for (int w0 = (blockIdx.x * WARPS_PER_BLOCK + (threadIdx.x >> 5)) * PER; w0 < count; w0 += warps * PER) {
+        int si = -1, vi = -1;
+        bool need = false;
+        if (lane < PER && w0 + lane < count) {
+            const int2 item = D.drown[from_list ? D.wlExact[w0 + lane] : w0 + lane];
+            si = item.x;
+            vi = item.y;
+            need = valid_id(D, si) && valid_id(D, vi) && hist_state(D, vi, si) == 2;
+        }
+        unsigned todo = __ballot_sync(0xffffffffu, need);
+    while (todo) {
+        const int src = __ffs(todo) - 1;
+        todo &= todo - 1;
+        const int s = __shfl_sync(0xffffffffu, si, src), v = __shfl_sync(0xffffffffu, vi, src);
+        const int w = w0 + src;
         __syncwarp();  // the previous item's shared-memory reads are done
-        const int idx = from_list ? D.wlExact[w] : w;
-        const int2 item = D.drown[idx];
-        const int s = item.x, v = item.y;
-        if (!valid_id(D, s) || !valid_id(D, v)) continue;
-        // a proof is needed only while v's star still links back to s
-        if (hist_state(D, v, s) != 2) continue;
         const StarHdr h = D.hdr[s];
         if (h.ntri == 0) continue;
         const StarView V = star_view(D, s);
@@ -1280,6 +1294,7 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK, EXACT ? 4 : PROOF_BLOCKS
             atomicAdd(&D.ctr->proofs_total, 1ull);
             if (anyovf) atomicOr(&D.ctr->overflow, 1);
         }
+    }
     }
 }
 
@@ -1837,7 +1852,7 @@ void launch_proof(const Launch& L, const Dev& D, int count) {
     // filter-only pass, then the exact pass over what it left (its count is
     // read on the device, so no host round trip), then the queue is emptied
     // for the star kernels
-    k_proof<false><<<star_blocks(count), 32 * WARPS_PER_BLOCK, 0, L.stream>>>(D, count);
+    k_proof<false><<<star_blocks((count + 31) / 32), 32 * WARPS_PER_BLOCK, 0, L.stream>>>(D, count);
     k_proof<true><<<star_blocks(count, WARPS_PER_BLOCK, 4), 32 * WARPS_PER_BLOCK, 0, L.stream>>>(D, count);
     cudaMemsetAsync(&D.ctr->exact_next, 0, sizeof(int), L.stream);
     *L.launches += 2;
