@@ -240,11 +240,14 @@ __device__ __forceinline__ int pred4(double3 a, double3 b, double3 c, double3 d,
 // coordinates for its big-integer fallback. Both give the exact sign or,
 // filter-only, 0 (undecided).
 // orient4(a, b, c, star, p): p against the link triangle (a, b, c)
+// (`bound`: the filter-only kernels' bound for every coordinate the star has
+// cached, orient4_static_bound of their largest magnitude)
 template <bool EXACT>
 __device__ __forceinline__ int pred_beneath(double3 a, double3 b, double3 c, double3 ps, double3 pp, int ia, int ib,
-                                            int ic, int is, int ip, const PredSink& sink, unsigned* exact) {
+                                            int ic, int is, int ip, const PredSink& sink, unsigned* exact,
+                                            double bound) {
     if (EXACT) return orient4(a, b, c, ps, pp, ia, ib, ic, is, ip, sink, exact);
-    return -orient4_filter_rel(a, b, c, pp);  // the star's point as the base: rows a, b, c, p swap two points
+    return -orient4_filter_rel_bounded(a, b, c, pp, bound);  // the star's point as the base: rows a, b, c, p swap two points
 }
 // orient4(l0, l1, l2, l3, star)
 template <bool EXACT>
@@ -291,6 +294,18 @@ __device__ __forceinline__ void ws_cache_coords(WS<C>& S, const Dev& D, int slot
     S.cx[cc] = p.x - base.x;
     S.cy[cc] = p.y - base.y;
     S.cz[cc] = p.z - base.z;
+}
+
+// filter bound for every coordinate the warp's star has cached (relative to
+// the star's point in the filter-only kernels), the same value in every lane
+template <class C>
+__device__ __forceinline__ double cache_bound(const WS<C>& S, int lane) {
+    double r = 0.0;
+    const int nc = min(S.ncoord, C::HM + 1);
+    for (int c = lane; c < nc; c += 32) r = fmax(r, fmax(fabs(S.cx[c]), fmax(fabs(S.cy[c]), fabs(S.cz[c]))));
+#pragma unroll
+    for (int o = 16; o; o >>= 1) r = fmax(r, __shfl_xor_sync(0xffffffffu, r, o));
+    return orient4_static_bound(r);
 }
 
 // Membership of v in star `star`: 0 = never inserted, 1 = in the history but
@@ -420,7 +435,7 @@ __device__ __forceinline__ int ws_hash_insert(WS<C>& S, int v, bool* fresh) {
 // when a filter-only kernel meets an undecided predicate (nothing changed).
 template <class C, bool EXACT>
 __device__ int warp_insert(WS<C>& S, int lane, int s, double3 ps, int sp, int gen, const PredSink& sink,
-                           unsigned* exact) {
+                           unsigned* exact, double bound) {
     using Idx = typename C::Idx;
     unsigned* err = sink.err;
     const double3 pp = wpt(S, sp);
@@ -437,7 +452,7 @@ __device__ int warp_insert(WS<C>& S, int lane, int s, double3 ps, int sp, int ge
             al = true;
             a = S.tv[0][t]; bb = S.tv[1][t]; c = S.tv[2][t];
             const int sg = pred_beneath<EXACT>(wpt(S, a), wpt(S, bb), wpt(S, c), ps, pp, wid(S, a), wid(S, bb),
-                                               wid(S, c), s, pid, sink, exact);
+                                               wid(S, c), s, pid, sink, exact, bound);
             b = sg < 0;
             und = sg == 0;
         }
@@ -476,7 +491,7 @@ __device__ int warp_insert(WS<C>& S, int lane, int s, double3 ps, int sp, int ge
                 al = true;
                 const int a = S.tv[0][t], bb = S.tv[1][t], c = S.tv[2][t];
                 const int sg = pred_beneath<EXACT>(wpt(S, a), wpt(S, bb), wpt(S, c), ps, pp, wid(S, a), wid(S, bb),
-                                                   wid(S, c), s, pid, sink, exact);
+                                                   wid(S, c), s, pid, sink, exact, bound);
                 b = sg < 0;
                 und = sg == 0;
             }
@@ -920,7 +935,9 @@ __global__ void __launch_bounds__(32 * C::WARPS, EXACT ? C::MINB : C::MINB_FAST)
         const int gen = 1;
         int l4[4] = {S.order[0], S.order[1], S.order[2], S.order[3]};
         int r = warp_cone<C, EXACT>(S, lane, s, ps, l4, gen, sink, exact);
-        for (int i = 4; i < nins && r >= 0; ++i) r = warp_insert<C, EXACT>(S, lane, s, ps, S.order[i], gen, sink, exact);
+        const double bound = EXACT ? 0.0 : cache_bound(S, lane);
+        for (int i = 4; i < nins && r >= 0; ++i)
+            r = warp_insert<C, EXACT>(S, lane, s, ps, S.order[i], gen, sink, exact, bound);
         if (r == -3 || r == -2) {
             if (lane == 0) {
                 if (r == -3) defer(D.wlExact, &D.ctr->exact_next, s);
@@ -996,8 +1013,9 @@ __global__ void __launch_bounds__(32 * C::WARPS, EXACT ? C::MINB : C::MINB_FAST)
         if (!outgrown) {
             if (lane == 0) S.nhist = nhist0 + nins;
             __syncwarp();
+            const double bound = EXACT ? 0.0 : cache_bound(S, lane);
             for (int i = 0; i < nins && !failed; ++i) {
-                const int r = warp_insert<C, EXACT>(S, lane, s, ps, S.order[i], gen, sink, exact);
+                const int r = warp_insert<C, EXACT>(S, lane, s, ps, S.order[i], gen, sink, exact, bound);
                 outgrown = r == -2;
                 undecided = r == -3;
                 failed = r < 0;
@@ -1091,15 +1109,16 @@ __device__ __forceinline__ const int* stage_ids(const StarView& V, int* smem, in
 }
 
 __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK, 16) k_emit(Dev D, int count) {
-    __shared__ int shh[WARPS_PER_BLOCK][HSLOTS];
     const int lane = threadIdx.x & 31;
     const int warps = gridDim.x * WARPS_PER_BLOCK;
     for (int w = blockIdx.x * WARPS_PER_BLOCK + (threadIdx.x >> 5); w < count; w += warps) {
-        __syncwarp();  // the previous item's shared-memory reads are done
         const int s = D.wlEmit[w];
         const StarHdr h = D.hdr[s];
         const StarView V = star_view(D, s);
-        const int* ids = stage_ids(V, shh[threadIdx.x >> 5], lane);
+        // ids of the fresh triangles' vertices straight from the history hash
+        // (after the first round a star has few fresh triangles, so staging
+        // the whole table would read far more than they need)
+        const int* ids = V.hh;
         bool ovf = false;
         for (int t = lane; t < h.ntri; t += 32) {
             const TriU T = tri_get(V, t);
