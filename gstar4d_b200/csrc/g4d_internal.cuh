@@ -99,6 +99,7 @@ struct Counters {
     int dbg_ids[5];
     int fix_next;         // tetra output: neighbour links written by the other side
     int block_pairs;      // workset pairs added from voxel blocks
+    int proof_next;       // drowned items of this round that need a proof
     unsigned long long cand_total;  // initial star insertions at most (sum over the worksets)
 };
 

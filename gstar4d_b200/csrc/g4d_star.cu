@@ -1201,51 +1201,58 @@ __global__ void k_requeue(Dev D, int count) {
 // containment proofs for drowned points (GDelPredKernels.cu:427-626)
 // --------------------------------------------------------------------------
 
+// A proof is needed only while v's star still links back to s, which most
+// drowned points' stars no longer do (2.5M proofs from about 35M drowned items
+// on the 8M cloud): k_proof_need checks every item, one per thread (the check
+// is a remote history probe, so many in flight), and lists those that need a
+// proof; the proof kernels take the list, one item per warp.
+__global__ void __launch_bounds__(256) k_proof_need(Dev D, const int2* __restrict__ items, int count,
+                                                   int2* __restrict__ need, int* __restrict__ nneed) {
+    const int lane = threadIdx.x & 31;
+    const int steps = (count + 31) & ~31;  // whole warps take part in the list appends
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < steps; i += gridDim.x * blockDim.x) {
+        int2 it = make_int2(-1, -1);
+        bool keep = false;
+        if (i < count) {
+            it = items[i];
+            keep = valid_id(D, it.x) && valid_id(D, it.y) && hist_state(D, it.y, it.x) == 2;
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        int base = 0;
+        if (lane == 0 && m) base = atomicAdd(nneed, __popc(m));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (keep) need[base + __popc(m & ((1u << lane) - 1u))] = it;
+    }
+}
+
+// Proofs of the listed items (count read on the device), one per warp.
 // EXACT = false: the FP64 filter alone; an item whose search meets an
 // undecided predicate is left untouched and its index queued on wlExact
 // (exact_next), for the exact kernel. EXACT = true: the exact predicates, over
-// the queued items (count read on the device), or over every item when the
-// queue overflowed (repeating a proof only repeats deduplicated requests).
+// the queued items, or over every item when the queue overflowed (repeating a
+// proof only repeats deduplicated requests).
 template <bool EXACT>
-__global__ void __launch_bounds__(32 * WARPS_PER_BLOCK, EXACT ? 4 : PROOF_BLOCKS) k_proof(Dev D, int count) {
-    __shared__ int shh[WARPS_PER_BLOCK][HSLOTS];
+__global__ void __launch_bounds__(32 * WARPS_PER_BLOCK, EXACT ? 4 : PROOF_BLOCKS)
+    k_proof(Dev D, const int2* __restrict__ items, const int* __restrict__ nitems) {
     const int lane = threadIdx.x & 31;
     const PredSink sink = sink_of(D);
     unsigned* err = sink.err;
     unsigned* exact = &D.ctr->exact;
     const int warps = gridDim.x * WARPS_PER_BLOCK;
+    int count = *(volatile const int*)nitems;
     bool from_list = false;
     if (EXACT) {
         const int queued = *(volatile int*)&D.ctr->exact_next;
         from_list = queued <= D.n;
         if (from_list) count = queued;
     }
-    // A proof is needed only while v's star still links back to s, which most
-    // drowned points' stars no longer do: the filter-only kernel takes 32 items
-    // per warp at a time, every lane checks one, and the warp then searches the
-    // proofs of those left. The exact kernel's items (the few the filter could
-    // not decide, each costly) go one per warp.
-    constexpr int PER = EXACT ? 1 : 32;
-    for (int w0 = (blockIdx.x * WARPS_PER_BLOCK + (threadIdx.x >> 5)) * PER; w0 < count; w0 += warps * PER) {
-        int si = -1, vi = -1;
-        bool need = false;
-        if (lane < PER && w0 + lane < count) {
-            const int2 item = D.drown[from_list ? D.wlExact[w0 + lane] : w0 + lane];
-            si = item.x;
-            vi = item.y;
-            need = valid_id(D, si) && valid_id(D, vi) && hist_state(D, vi, si) == 2;
-        }
-        unsigned todo = __ballot_sync(0xffffffffu, need);
-    while (todo) {
-        const int src = __ffs(todo) - 1;
-        todo &= todo - 1;
-        const int s = __shfl_sync(0xffffffffu, si, src), v = __shfl_sync(0xffffffffu, vi, src);
-        const int w = w0 + src;
-        __syncwarp();  // the previous item's shared-memory reads are done
+    for (int w = blockIdx.x * WARPS_PER_BLOCK + (threadIdx.x >> 5); w < count; w += warps) {
+        const int2 item = items[from_list ? D.wlExact[w] : w];
+        const int s = item.x, v = item.y;
         const StarHdr h = D.hdr[s];
         if (h.ntri == 0) continue;
         const StarView V = star_view(D, s);
-        const int* ids = stage_ids(V, shh[threadIdx.x >> 5], lane);
+        const int* ids = V.hh;  // the vertices' ids straight from the history hash
         const double3 ps = gpt(D, s), pv = gpt(D, v);
         const int ex = ids[tri_get(V, 0).v[0]] & (int)HID;
         const double3 pe = gpt(D, ex);
@@ -1313,7 +1320,6 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK, EXACT ? 4 : PROOF_BLOCKS
             atomicAdd(&D.ctr->proofs_total, 1ull);
             if (anyovf) atomicOr(&D.ctr->overflow, 1);
         }
-    }
     }
 }
 
@@ -1868,13 +1874,20 @@ void launch_reroute(const Launch& L, const Dev& D, int count) {
 }
 
 void launch_proof(const Launch& L, const Dev& D, int count) {
-    // filter-only pass, then the exact pass over what it left (its count is
-    // read on the device, so no host round trip), then the queue is emptied
-    // for the star kernels
-    k_proof<false><<<star_blocks((count + 31) / 32), 32 * WARPS_PER_BLOCK, 0, L.stream>>>(D, count);
-    k_proof<true><<<star_blocks(count, WARPS_PER_BLOCK, 4), 32 * WARPS_PER_BLOCK, 0, L.stream>>>(D, count);
+    // the items that need a proof into the next round's drowned list (free
+    // until the insertion kernels refill it), then the filter-only pass over
+    // them, then the exact pass over what it left (counts read on the device,
+    // so no host round trip), then the queue is emptied for the star kernels
+    int* nneed = &D.ctr->proof_next;
+    cudaMemsetAsync(nneed, 0, sizeof(int), L.stream);
+    int b = (count + 255) / 256;
+    if (b > 148 * 16) b = 148 * 16;
+    k_proof_need<<<b < 1 ? 1 : b, 256, 0, L.stream>>>(D, D.drown, count, D.drownNext, nneed);
+    const int upper = count / 4 + 1;  // grid of the proof kernels (grid-stride over the device count)
+    k_proof<false><<<star_blocks(upper), 32 * WARPS_PER_BLOCK, 0, L.stream>>>(D, D.drownNext, nneed);
+    k_proof<true><<<star_blocks(upper, WARPS_PER_BLOCK, 4), 32 * WARPS_PER_BLOCK, 0, L.stream>>>(D, D.drownNext, nneed);
     cudaMemsetAsync(&D.ctr->exact_next, 0, sizeof(int), L.stream);
-    *L.launches += 2;
+    *L.launches += 3;
 }
 
 void launch_check(const Launch& L, const Dev& D, unsigned long long* bad) {
