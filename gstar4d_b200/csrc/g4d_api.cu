@@ -923,6 +923,9 @@ g4d_status run_wave(g4d_ctx* ctx, const double* d_xyz, const int64_t* offs, cons
             launch_pairs_stack(L, D, gA + S.vox, map + S.vox, S.G, S.K, ckey, ctx->b[B_CID].as<int>(), cs + S.col,
                                ce + S.col);
         launch_missing_u64(L, D, skey);
+        if (ctx->block_k > 0)
+            launch_block_pairs_batch(L, D, gA, map, skey, d_slotG, d_slotVox, ctx->block_k);
+        launch_workset_total(L, D);
         bool again = false;
         st = worksets_fit(ctx, D, attempt, &again);
         if (st) return st;

@@ -47,33 +47,50 @@ __device__ __forceinline__ float dist2(double4 a, double4 b) {
     return (float)(dx * dx + dy * dy + dz * dz);
 }
 
-__global__ void __launch_bounds__(128) k_block_sel(Dev D, const uint32_t* __restrict__ grid,
-                                                   const int* __restrict__ map, int k_sel, int* __restrict__ sel,
-                                                   float* __restrict__ thr) {
+// Where point s's grid lies: one cloud (width D.G at offset 0), or a batch,
+// where point s belongs to slot key >> 30, whose grid has width slotG[k] and
+// starts at voxel slotVox[k] of the stacked grids.
+struct GridOf {
+    const int* slotG;        // null: one cloud
+    const long long* slotVox;
+    __device__ __forceinline__ void locate(const Dev& D, unsigned long long key, int* G, size_t* base) const {
+        if (!slotG) { *G = D.G; *base = 0; return; }
+        const int k = (int)(key >> 30);
+        *G = slotG[k];
+        *base = (size_t)slotVox[k];
+    }
+};
+
+template <class KeyT>
+__global__ void __launch_bounds__(128) k_block_sel(Dev D, const KeyT* __restrict__ keys, GridOf go,
+                                                   const uint32_t* __restrict__ grid, const int* __restrict__ map,
+                                                   int k_sel, int* __restrict__ sel, float* __restrict__ thr) {
     __shared__ int ids[4][BLOCK_MAX];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int G = D.G;
     const unsigned full = 0xffffffffu;
     for (int s = blockIdx.x * 4 + w; s < D.n; s += gridDim.x * 4) {
         // only points of voxels with several points select: elsewhere the
         // Voronoi pairs already join every occupied neighbouring voxel
-        const uint32_t ks = D.mkey[s];
-        if (!((s > 0 && D.mkey[s - 1] == ks) || (s + 1 < D.n && D.mkey[s + 1] == ks))) {
+        const KeyT ks = keys[s];
+        if (!((s > 0 && keys[s - 1] == ks) || (s + 1 < D.n && keys[s + 1] == ks))) {
             if (lane == 0) thr[s] = -1.0f;
             continue;
         }
+        int G;
+        size_t gbase;
+        go.locate(D, (unsigned long long)ks, &G, &gbase);
         const uint32_t e = D.vox[s];
         int lead = 0, run = 0;
         if (lane < 27) {
             const int o = c_block_order[lane];
             const int xx = (int)vx(e) + o % 3 - 1, yy = (int)vy(e) + (o / 3) % 3 - 1, zz = (int)vz(e) + o / 9 - 1;
             if (xx >= 0 && yy >= 0 && zz >= 0 && xx < G && yy < G && zz < G) {
-                const size_t u = ((size_t)zz * G + yy) * G + xx;
+                const size_t u = gbase + ((size_t)zz * G + yy) * G + xx;
                 if (grid[u] == enc_vox((uint32_t)xx, (uint32_t)yy, (uint32_t)zz)) {
                     lead = map[u];
-                    const uint32_t k = D.mkey[lead];
+                    const KeyT k = keys[lead];
                     run = 1;
-                    while (run < BLOCK_RUN && lead + run < D.n && D.mkey[lead + run] == k) ++run;
+                    while (run < BLOCK_RUN && lead + run < D.n && keys[lead + run] == k) ++run;
                 }
             }
         }
@@ -189,7 +206,18 @@ void launch_block_pairs(const Launch& L, const Dev& D, const uint32_t* grid, con
     int b = (D.n + 3) / 4;
     if (b > 148 * 16) b = 148 * 16;
     float* thr = reinterpret_cast<float*>(D.inboxCount);
-    k_block_sel<<<b, 128, 0, L.stream>>>(D, grid, map, k_sel, D.inbox, thr);
+    k_block_sel<uint32_t><<<b, 128, 0, L.stream>>>(D, D.mkey, GridOf{nullptr, nullptr}, grid, map, k_sel, D.inbox, thr);
+    k_block_push<<<b, 128, 0, L.stream>>>(D, D.inbox, thr);
+    *L.launches += 2;
+}
+
+void launch_block_pairs_batch(const Launch& L, const Dev& D, const uint32_t* grids, const int* maps,
+                              const unsigned long long* skey, const int* slotG, const long long* slotVox, int k_sel) {
+    int b = (D.n + 3) / 4;
+    if (b > 148 * 16) b = 148 * 16;
+    float* thr = reinterpret_cast<float*>(D.inboxCount);
+    k_block_sel<unsigned long long><<<b, 128, 0, L.stream>>>(D, skey, GridOf{slotG, slotVox}, grids, maps, k_sel,
+                                                             D.inbox, thr);
     k_block_push<<<b, 128, 0, L.stream>>>(D, D.inbox, thr);
     *L.launches += 2;
 }

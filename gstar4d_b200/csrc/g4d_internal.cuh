@@ -276,6 +276,10 @@ void launch_missing_u64(const Launch& L, const Dev& D, const unsigned long long*
 // workset pairs of each point with its k_sel nearest points of the 3x3x3 voxel
 // block (single clouds; the insertion-request arrays serve as scratch)
 void launch_block_pairs(const Launch& L, const Dev& D, const uint32_t* grid, const int* map, int k_sel);
+// the same over a batch pass: point i of slot k = skey >> 30 in the grid at
+// slotVox[k] (width slotG[k]) of the stacked grids and maps
+void launch_block_pairs_batch(const Launch& L, const Dev& D, const uint32_t* grids, const int* maps,
+                              const unsigned long long* skey, const int* slotG, const long long* slotVox, int k_sel);
 // ctr->cand_total = sum over stars of the initial insertions they can make
 // (the workset, pumped up to MIN_WORKSET): the initial build's drowned points
 void launch_workset_total(const Launch& L, const Dev& D);

@@ -1099,15 +1099,6 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_promote(Dev D, int cou
 // each other (GDelKernels.cu:818-939)
 // --------------------------------------------------------------------------
 
-// history ids of star s by slot: small stars are copied to shared memory,
-// large ones are read in place
-__device__ __forceinline__ const int* stage_ids(const StarView& V, int* smem, int lane) {
-    if (V.large) return V.hh;
-    for (int k = lane; k < HSLOTS; k += 32) smem[k] = V.hh[k] & (int)HID;
-    __syncwarp();
-    return smem;
-}
-
 __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK, 16) k_emit(Dev D, int count) {
     const int lane = threadIdx.x & 31;
     const int warps = gridDim.x * WARPS_PER_BLOCK;
@@ -1453,7 +1444,6 @@ __global__ void k_check(Dev D, unsigned long long* bad) {
 // its count from the device (or every star when the queue overflowed).
 template <bool EXACT>
 __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK, EXACT ? 1 : 8) k_tet_count(Dev D, int* cnt) {
-    __shared__ int shh[WARPS_PER_BLOCK][HSLOTS];
     const int lane = threadIdx.x & 31;
     const PredSink sink = sink_of(D);
     const int warps = gridDim.x * WARPS_PER_BLOCK;
@@ -1466,10 +1456,9 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK, EXACT ? 1 : 8) k_tet_cou
     }
     for (int w = blockIdx.x * WARPS_PER_BLOCK + (threadIdx.x >> 5); w < count; w += warps) {
         const int s = from_list ? D.wlExact[w] : w;
-        __syncwarp();  // the previous star's shared-memory reads are done
         const StarHdr h = D.hdr[s];
         const StarView V = star_view(D, s);
-        const int* ids = stage_ids(V, shh[threadIdx.x >> 5], lane);
+        const int* ids = V.hh;  // the link vertices' ids straight from the history hash
         const double3 ps = gpt(D, s);
         // (an undecided sign leaves the star to the exact kernel, which
         // rewrites every kept bit and the count)
@@ -1705,7 +1694,6 @@ __device__ __forceinline__ void write_star_small(const Dev& D, const int* base, 
 
 __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_tet_write(Dev D, const int* base, g4d_tet* tets,
                                                                     const int* sorted_to_input, int4* face) {
-    __shared__ int shh[WARPS_PER_BLOCK][HSLOTS];
     // large stars: triangle ranks; small stars: write_star_small's buffer
     __shared__ __align__(16) uint16_t srank[WARPS_PER_BLOCK][LTSTRIDE];
     static_assert(256 + 4 * TMAX * sizeof(int) <= LTSTRIDE * sizeof(uint16_t), "small-star output buffer");
@@ -1716,7 +1704,7 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_tet_write(Dev D, const
         __syncwarp();  // the previous star's shared-memory reads are done
         const StarHdr h = D.hdr[s];
         const StarView V = star_view(D, s);
-        const int* ids = stage_ids(V, shh[threadIdx.x >> 5], lane);
+        const int* ids = V.hh;  // the link vertices' ids straight from the history hash
         if (!V.large)
             write_star_small(D, base, tets, sorted_to_input, face, s, h.ntri, ids, static_cast<const uint2*>(V.tri),
                              reinterpret_cast<uint8_t*>(rank), lane);
