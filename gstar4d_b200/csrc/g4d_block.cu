@@ -13,13 +13,16 @@
 // gets the other points of those voxels when they select it.)
 //
 // Splaying needs symmetric worksets (b in a's history means a in b's, or on
-// its way), so every pair is pushed both ways, and exactly once: the selection
+// its way), so every pair is pushed both ways, and never twice: the selection
 // of a point is "distance at most its threshold" (the K-th smallest block
 // distance), and the pair (s, v) is pushed by s when v is in s's selection and
 // either v > s or s is beyond v's threshold, else by v. The squared distance of
 // a pair is the same float from both sides (the differences only change sign).
-// Which pairs are added only changes the work splaying has left: the stars are
-// decided by the exact predicates whatever their candidates.
+// Every selected pair is pushed once, except where the side the rule leaves it
+// to never gathered the other (beyond the caps below); such a pair is left to
+// splaying. Which pairs are added only changes the work splaying has left: the
+// stars are decided by the exact predicates whatever their candidates
+// (tests/test_block_rule.py restates the rule and checks it on the CPU).
 //
 // k_block_sel: warp per point; the block's occupied voxels (a voxel whose site
 //   is itself; its points are the run of equal Morton keys from its leader) in
