@@ -509,7 +509,7 @@ def main():
             "metric": METRIC, "value": round(value, 3), "unit": "Mpts/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": dict(cfg, method="plain PBA stars (learned proposal in learned_proposal)",
+            "config": dict(cfg, method="plain PBA stars with voxel-block workset pairs (learned proposal in learned_proposal)",
                            l2="256 MB buffer written between timed steps", parallelism="replicas"),
             "e2e": {"value": round(e2e, 3), "unit": "Mpts/s", "h2d_bytes_per_step": int(n * 24),
                     "d2h_bytes_per_step": int(ntet_e2e * 32)},
